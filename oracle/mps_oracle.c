@@ -1,0 +1,1093 @@
+/*
+ * mps_oracle.c -- CPU restatement of the reference MPS time step (checker).
+ *
+ * TEST INFRASTRUCTURE ONLY: see mps_oracle.h.  Built twice by oracle/Makefile
+ * (MPS_DIM=3 -> liboracle3d.so, MPS_DIM=2 -> liboracle2d.so) with
+ * -O2 -ffp-contract=off.  Citations name the reference function each block
+ * restates; 3P = mps_fluid3D_parallel, 2D = mps_fluid2D.
+ *
+ * Floating-point order is part of the contract: every sum runs in the same
+ * order and association as the reference, so that outputs are bit-identical
+ * to the reference built from its own sources.
+ */
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "mps_oracle.h"
+
+#define D MPS_DIM
+
+static int    g_last_iters = 0;
+static double g_last_resid = 0.0;
+
+int    oracle_last_iterations(void) { return g_last_iters; }
+double oracle_last_residual(void)   { return g_last_resid; }
+
+/* Squared distance accumulated as ((0 + dx^2) + dy^2) + dz^2 with dx = pj - pi,
+ * the order of every distance loop in the reference (e.g. 3P operators.c:28-32). */
+static inline double dist2(const double *pi, const double *pj)
+{
+    double acc = 0.0;
+    for (int d = 0; d < D; d++) {
+        double t = pj[d] - pi[d];
+        acc += t * t;
+    }
+    return acc;
+}
+
+static inline double dist2_vec(const double *pi, const double *pj, double *dr)
+{
+    double acc = 0.0;
+    for (int d = 0; d < D; d++) {
+        dr[d] = pj[d] - pi[d];
+        acc += dr[d] * dr[d];
+    }
+    return acc;
+}
+
+/* 3P kernel.c:12-20: w = re/r - 1 with r clamped below at 0.01*l0, 0 beyond re. */
+double oracle_kernel_weight(double r, double re, const SimConfig *cfg)
+{
+    if (r >= re) return 0.0;
+    double rmin = 0.01 * cfg->particle_distance;
+    double rr = (r < rmin) ? rmin : r;
+    return re / rr - 1.0;
+}
+#define KW(r, re) oracle_kernel_weight((r), (re), cfg)
+
+/* ------------------------------------------------------------------ */
+/* Initial parameters n0, lambda, N0  (3P particle.c:69-221)           */
+/* ------------------------------------------------------------------ */
+
+/* Serial semantics of the reference: first strictly larger n0_i in particle
+ * index order wins and carries its lambda numerator/denominator.  (The OpenMP
+ * build merges per-thread maxima with the same strict '>' and equals this
+ * unless two n0_i are bitwise equal.) */
+static void finish_initial_params(ParticleSystem *ps, const SimConfig *cfg, int found,
+                                  double best_n0, double best_num, double best_den)
+{
+    double re_lap = cfg->influence_radius_lap;
+    if (!found) {
+        ps->n0 = 1.0;
+        ps->lambda = 1.0;
+        return;
+    }
+    ps->n0 = best_n0;
+    if (cfg->use_analytical_lambda)
+        ps->lambda = re_lap * re_lap * (double)D * (double)(D - 1)
+                   / ((double)(D + 1) * (double)(D + 2));
+    else
+        ps->lambda = (best_den > 1.0e-10) ? best_num / best_den : 1.0;
+}
+
+static int initial_count_for(const ParticleSystem *ps, int i, double re_n2)
+{
+    int c = 0;
+    for (int j = 0; j < ps->num; j++) {
+        if (j == i) continue;
+        if (dist2(ps->particles[i].pos, ps->particles[j].pos) < re_n2) c++;
+    }
+    return c;
+}
+
+void oracle_calc_initial_params(ParticleSystem *ps, const SimConfig *cfg)
+{
+    double re_n = cfg->influence_radius_n, re_lap = cfg->influence_radius_lap;
+    double best_n0 = 0.0, best_num = 0.0, best_den = 0.0;
+    int found = 0;
+
+    for (int i = 0; i < ps->num; i++) {
+        const Particle *pi = &ps->particles[i];
+        if (pi->type != MPS_FLUID) continue;
+        double n0_i = 0.0, num_i = 0.0, den_i = 0.0;
+        for (int j = 0; j < ps->num; j++) {
+            if (j == i) continue;
+            double r2 = dist2(pi->pos, ps->particles[j].pos);
+            double r = sqrt(r2);
+            double wn = KW(r, re_n);
+            if (wn > 0.0) n0_i += wn;
+            double wl = KW(r, re_lap);
+            if (wl > 0.0) { num_i += r2 * wl; den_i += wl; }
+        }
+        if (n0_i > best_n0) { best_n0 = n0_i; best_num = num_i; best_den = den_i; found = 1; }
+    }
+    finish_initial_params(ps, cfg, found, best_n0, best_num, best_den);
+    if (!found) return;   /* the reference returns before N0 (3P particle.c:159-164) */
+
+    if (cfg->surface_detection_method == 1) {
+        int best = 0;
+        double re_n2 = re_n * re_n;
+        for (int i = 0; i < ps->num; i++) {
+            if (ps->particles[i].type != MPS_FLUID) continue;
+            int c = initial_count_for(ps, i, re_n2);
+            if (c > best) best = c;
+        }
+        ps->n0_count = best;
+    }
+}
+
+/* Same result bit for bit, O(N*K) instead of O(N^2): candidates come from a
+ * uniform grid over the particles' own bounding box (so no particle is left
+ * out), and each particle's contributions are summed in ascending j, the
+ * reference's loop order.  Terms with w <= 0 are skipped by the reference too,
+ * and they are the only pairs a radius test drops. */
+typedef struct { int j; double r2; } Cand;
+
+static int cand_cmp(const void *a, const void *b)
+{
+    int x = ((const Cand *)a)->j, y = ((const Cand *)b)->j;
+    return (x > y) - (x < y);
+}
+
+void oracle_calc_initial_params_cells(ParticleSystem *ps, const SimConfig *cfg)
+{
+    int n = ps->num;
+    double re_n = cfg->influence_radius_n, re_lap = cfg->influence_radius_lap;
+    double rmax = re_n > re_lap ? re_n : re_lap;
+    double cs = rmax * (1.0 + 1.0e-9);
+    double lo[D], hi[D];
+    int dims[D];
+    long long ncell = 1;
+    for (int d = 0; d < D; d++) { lo[d] = INFINITY; hi[d] = -INFINITY; }
+    for (int i = 0; i < n; i++)
+        for (int d = 0; d < D; d++) {
+            double v = ps->particles[i].pos[d];
+            if (v < lo[d]) lo[d] = v;
+            if (v > hi[d]) hi[d] = v;
+        }
+    /* Non-finite coordinates would break the grid; fall back to all pairs. */
+    for (int d = 0; d < D; d++) {
+        if (!isfinite(lo[d]) || !isfinite(hi[d])) { oracle_calc_initial_params(ps, cfg); return; }
+        dims[d] = (int)((hi[d] - lo[d]) / cs) + 1;
+        ncell *= dims[d];
+    }
+    if (ncell > 200000000LL) { oracle_calc_initial_params(ps, cfg); return; }
+
+    int *cell_of = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    int *start = (int *)calloc((size_t)ncell + 1, sizeof(int));
+    int *order = (int *)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    Cand *cand = NULL;
+    int cand_cap = 0;
+    if (!cell_of || !start || !order) {
+        free(cell_of); free(start); free(order);
+        oracle_calc_initial_params(ps, cfg);
+        return;
+    }
+    for (int i = 0; i < n; i++) {
+        long long c = 0;
+        for (int d = D - 1; d >= 0; d--) {
+            int k = (int)((ps->particles[i].pos[d] - lo[d]) / cs);
+            if (k >= dims[d]) k = dims[d] - 1;
+            c = c * dims[d] + k;
+        }
+        cell_of[i] = (int)c;
+        start[c + 1]++;
+    }
+    for (long long c = 0; c < ncell; c++) start[c + 1] += start[c];
+    {
+        int *fill = (int *)malloc(sizeof(int) * (size_t)ncell);
+        memcpy(fill, start, sizeof(int) * (size_t)ncell);
+        for (int i = 0; i < n; i++) order[fill[cell_of[i]]++] = i;
+        free(fill);
+    }
+
+    double best_n0 = 0.0, best_num = 0.0, best_den = 0.0;
+    int found = 0, best_cnt = 0;
+    double re_n2 = re_n * re_n, rmax2 = rmax * rmax;
+    for (int i = 0; i < n; i++) {
+        const Particle *pi = &ps->particles[i];
+        if (pi->type != MPS_FLUID) continue;
+        int ci[D];
+        long long c = cell_of[i];
+        for (int d = 0; d < D; d++) { ci[d] = (int)(c % dims[d]); c /= dims[d]; }
+        int nc = 0;
+        int lo_k[D], hi_k[D], k[D];
+        for (int d = 0; d < D; d++) {
+            lo_k[d] = ci[d] > 0 ? ci[d] - 1 : 0;
+            hi_k[d] = ci[d] < dims[d] - 1 ? ci[d] + 1 : dims[d] - 1;
+            k[d] = lo_k[d];
+        }
+        for (;;) {
+            long long cc = 0;
+            for (int d = D - 1; d >= 0; d--) cc = cc * dims[d] + k[d];
+            for (int s = start[cc]; s < start[cc + 1]; s++) {
+                int j = order[s];
+                if (j == i) continue;
+                double r2 = dist2(pi->pos, ps->particles[j].pos);
+                /* keep every pair that can carry a positive weight or count */
+                if (!(r2 < rmax2) && !(sqrt(r2) < rmax)) continue;
+                if (nc == cand_cap) {
+                    cand_cap = cand_cap ? 2 * cand_cap : 1024;
+                    cand = (Cand *)realloc(cand, sizeof(Cand) * (size_t)cand_cap);
+                }
+                cand[nc].j = j;
+                cand[nc].r2 = r2;
+                nc++;
+            }
+            int d = 0;
+            while (d < D && ++k[d] > hi_k[d]) { k[d] = lo_k[d]; d++; }
+            if (d == D) break;
+        }
+        qsort(cand, (size_t)nc, sizeof(Cand), cand_cmp);
+        double n0_i = 0.0, num_i = 0.0, den_i = 0.0;
+        int cnt = 0;
+        for (int q = 0; q < nc; q++) {
+            double r2 = cand[q].r2;
+            double r = sqrt(r2);
+            double wn = KW(r, re_n);
+            if (wn > 0.0) n0_i += wn;
+            double wl = KW(r, re_lap);
+            if (wl > 0.0) { num_i += r2 * wl; den_i += wl; }
+            if (r2 < re_n2) cnt++;
+        }
+        if (n0_i > best_n0) { best_n0 = n0_i; best_num = num_i; best_den = den_i; found = 1; }
+        if (cnt > best_cnt) best_cnt = cnt;
+    }
+    finish_initial_params(ps, cfg, found, best_n0, best_num, best_den);
+    if (found && cfg->surface_detection_method == 1) ps->n0_count = best_cnt;
+    free(cand); free(cell_of); free(start); free(order);
+}
+
+/* ------------------------------------------------------------------ */
+/* Cell linked list and neighbour search (3P neighbor_search.c:92-240) */
+/* ------------------------------------------------------------------ */
+
+int oracle_cell_list_init(CellList *cl, int num_particles, double re,
+                          const double *domain_min, const double *domain_max)
+{
+    double margin = 4.0 * re;
+    cl->cell_size = re;
+    for (int d = 0; d < D; d++) cl->origin[d] = domain_min[d] - margin;
+    cl->nx = (int)(((domain_max[0] + margin) - cl->origin[0]) / re) + 2;
+    cl->ny = (int)(((domain_max[1] + margin) - cl->origin[1]) / re) + 2;
+#if D == 3
+    cl->nz = (int)(((domain_max[2] + margin) - cl->origin[2]) / re) + 2;
+    cl->total_cells = cl->nx * cl->ny * cl->nz;
+#else
+    cl->total_cells = cl->nx * cl->ny;
+#endif
+    cl->head = (int *)malloc(sizeof(int) * (size_t)cl->total_cells);
+    cl->next = (int *)malloc(sizeof(int) * (size_t)(num_particles > 0 ? num_particles : 1));
+    return (cl->head && cl->next) ? 0 : -1;
+}
+
+/* Cell coordinate of a position, (int) truncation of (p - origin) * (1/cs)
+ * exactly as 3P neighbor_search.c:155,171-173.  Returns 0 when outside. */
+static int cell_coords(const CellList *cl, double cs_inv, const double *p, int *c)
+{
+    int lim[D];
+    lim[0] = cl->nx; lim[1] = cl->ny;
+#if D == 3
+    lim[2] = cl->nz;
+#endif
+    for (int d = 0; d < D; d++) {
+        double t = (p[d] - cl->origin[d]) * cs_inv;
+        /* (int) of NaN or of an out-of-range value is undefined in C; x86
+         * yields INT_MIN, which the reference's range test rejects.  Make
+         * that rejection explicit. */
+        if (!(t > -1.0 && t < 2147483647.0)) return 0;
+        c[d] = (int)t;
+        if (c[d] < 0 || c[d] >= lim[d]) return 0;
+    }
+    return 1;
+}
+
+static int cell_linear(const CellList *cl, const int *c)
+{
+#if D == 3
+    return (c[2] * cl->ny + c[1]) * cl->nx + c[0];
+#else
+    return c[1] * cl->nx + c[0];
+#endif
+}
+
+int oracle_neighbor_search(NeighborList *nl, const ParticleSystem *ps, CellList *cl, double re)
+{
+    int n = ps->num, maxnb = nl->max_neighbors;
+    double re2 = re * re, cs_inv = 1.0 / cl->cell_size;
+    memset(nl->count, 0, sizeof(int) * (size_t)n);
+    for (int c = 0; c < cl->total_cells; c++) cl->head[c] = -1;
+
+    /* Phase 1: prepend each particle to its cell; within a cell the chain
+     * therefore runs in descending particle index. */
+    for (int i = 0; i < n; i++) {
+        int c[D];
+        cl->next[i] = -1;
+        if (ps->particles[i].type == MPS_GHOST) continue;
+        if (!cell_coords(cl, cs_inv, ps->particles[i].pos, c)) continue;
+        int ci = cell_linear(cl, c);
+        cl->next[i] = cl->head[ci];
+        cl->head[ci] = i;
+    }
+
+    /* Phase 2: scan the 3^D block of cells (z, then y, then x outermost to
+     * innermost) and keep pairs with r2 < re^2. */
+    int lim[D];
+    lim[0] = cl->nx; lim[1] = cl->ny;
+#if D == 3
+    lim[2] = cl->nz;
+#endif
+    for (int i = 0; i < n; i++) {
+        int c[D];
+        if (ps->particles[i].type == MPS_GHOST) continue;
+        if (!cell_coords(cl, cs_inv, ps->particles[i].pos, c)) continue;
+        int lo[D], hi[D];
+        for (int d = 0; d < D; d++) {
+            lo[d] = c[d] > 0 ? c[d] - 1 : 0;
+            hi[d] = c[d] < lim[d] - 1 ? c[d] + 1 : lim[d] - 1;
+        }
+        int cnt = 0;
+        int *row = nl->neighbors + (size_t)i * (size_t)maxnb;
+#if D == 3
+        for (int z = lo[2]; z <= hi[2]; z++)
+#endif
+        for (int y = lo[1]; y <= hi[1]; y++)
+        for (int x = lo[0]; x <= hi[0]; x++) {
+#if D == 3
+            int cc[3] = {x, y, z};
+#else
+            int cc[2] = {x, y};
+#endif
+            for (int j = cl->head[cell_linear(cl, cc)]; j >= 0; j = cl->next[j]) {
+                if (j == i || ps->particles[j].type == MPS_GHOST) continue;
+                if (dist2(ps->particles[i].pos, ps->particles[j].pos) < re2) {
+                    if (cnt >= maxnb) return -(i + 1);   /* reference: exit(1) */
+                    row[cnt++] = j;
+                }
+            }
+        }
+        nl->count[i] = cnt;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* Particle operators (3P operators.c)                                 */
+/* ------------------------------------------------------------------ */
+
+#define NB(nl, i, k) ((nl)->neighbors[(size_t)(i) * (size_t)(nl)->max_neighbors + (k)])
+
+/* 3P operators.c:17-38 */
+void oracle_number_density(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg)
+{
+    double re = cfg->influence_radius_n;
+    for (int i = 0; i < ps->num; i++) {
+        Particle *pi = &ps->particles[i];
+        double s = 0.0;
+        for (int k = 0; k < nl->count[i]; k++) {
+            const Particle *pj = &ps->particles[NB(nl, i, k)];
+            s += KW(sqrt(dist2(pi->pos, pj->pos)), re);
+        }
+        pi->n = s;
+    }
+}
+
+/* 3P operators.c:50-85: acc += (nu * 2d/(n0 lambda)) * sum (u_j - u_i) w */
+void oracle_viscosity(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg)
+{
+    double re = cfg->influence_radius_lap;
+    double coeff = 2.0 * D / (ps->n0 * ps->lambda);
+    double nu = cfg->viscosity;
+    for (int i = 0; i < ps->num; i++) {
+        Particle *pi = &ps->particles[i];
+        if (pi->type != MPS_FLUID) continue;
+        double lap[D];
+        for (int d = 0; d < D; d++) lap[d] = 0.0;
+        for (int k = 0; k < nl->count[i]; k++) {
+            const Particle *pj = &ps->particles[NB(nl, i, k)];
+            double w = KW(sqrt(dist2(pi->pos, pj->pos)), re);
+            for (int d = 0; d < D; d++) lap[d] += (pj->vel[d] - pi->vel[d]) * w;
+        }
+        for (int d = 0; d < D; d++) pi->acc[d] += nu * coeff * lap[d];
+    }
+}
+
+/* 3P operators.c:102-181: two passes, P_min then the gradient. */
+int oracle_pressure_gradient(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg)
+{
+    int n = ps->num, mode = cfg->cmps_gradient;
+    double re = cfg->influence_radius_lap;
+    double gcoef = (double)D / ps->n0;
+    double l0 = cfg->particle_distance, rho = cfg->density;
+    double *pmin = NULL;
+    if (mode != 2) {
+        pmin = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+        if (!pmin) return -1;
+        for (int i = 0; i < n; i++) {
+            double m = ps->particles[i].pressure;
+            for (int k = 0; k < nl->count[i]; k++) {
+                double pj = ps->particles[NB(nl, i, k)].pressure;
+                if (pj < m) m = pj;
+            }
+            pmin[i] = m;
+        }
+    }
+    for (int i = 0; i < n; i++) {
+        Particle *pi = &ps->particles[i];
+        if (pi->type != MPS_FLUID) continue;
+        double pim = pmin ? pmin[i] : 0.0;
+        double g[D];
+        for (int d = 0; d < D; d++) g[d] = 0.0;
+        for (int k = 0; k < nl->count[i]; k++) {
+            int j = NB(nl, i, k);
+            const Particle *pj = &ps->particles[j];
+            double dr[D];
+            double r2 = dist2_vec(pi->pos, pj->pos, dr);
+            if (r2 < l0 * l0 * 1.0e-12) continue;
+            double w = KW(sqrt(r2), re);
+            double dp;
+            if (mode == 1)      dp = pi->pressure + pj->pressure - pim - pmin[j];
+            else if (mode == 2) dp = pi->pressure + pj->pressure;
+            else                dp = pj->pressure - pim;
+            for (int d = 0; d < D; d++) g[d] += dp / r2 * dr[d] * w;
+        }
+        for (int d = 0; d < D; d++) pi->acc[d] = -gcoef * g[d] / rho;
+    }
+    free(pmin);
+    return 0;
+}
+
+/* 3P operators.c:188-199 */
+void oracle_clamp_pressure(ParticleSystem *ps)
+{
+    for (int i = 0; i < ps->num; i++)
+        if (ps->particles[i].type == MPS_FLUID && ps->particles[i].pressure < 0.0)
+            ps->particles[i].pressure = 0.0;
+}
+
+/* 3P operators.c:206-219 */
+void oracle_judge_free_surface(ParticleSystem *ps, double threshold)
+{
+    double lim = threshold * ps->n0;
+    for (int i = 0; i < ps->num; i++) {
+        Particle *p = &ps->particles[i];
+        p->on_surface = (p->type == MPS_FLUID && p->n < lim) ? 1 : 0;
+    }
+}
+
+/* 3P operators.c:226-246 */
+void oracle_neighbor_count(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg)
+{
+    double re2 = cfg->influence_radius_n * cfg->influence_radius_n;
+    for (int i = 0; i < ps->num; i++) {
+        int c = 0;
+        for (int k = 0; k < nl->count[i]; k++)
+            if (dist2(ps->particles[i].pos, ps->particles[NB(nl, i, k)].pos) < re2) c++;
+        ps->particles[i].neighbor_count = c;
+    }
+}
+
+/* 3P operators.c:253-267 */
+void oracle_judge_free_surface_by_count(ParticleSystem *ps, double beta)
+{
+    double lim = beta * ps->n0_count;
+    for (int i = 0; i < ps->num; i++) {
+        Particle *p = &ps->particles[i];
+        p->on_surface = (p->type == MPS_FLUID && p->neighbor_count < lim) ? 1 : 0;
+    }
+}
+
+/* Impulse of one candidate partner on v_i (3P operators.c:407-427). */
+static inline void collide_with(double *vi, const Particle *pi, const Particle *pj,
+                                double col2, double l0, double half1pe)
+{
+    double dr[D];
+    double r2 = dist2_vec(pi->pos, pj->pos, dr);
+    if (r2 >= col2) return;
+    double r = sqrt(r2);
+    if (r < 1.0e-12 * l0) return;
+    double vn = 0.0;
+    for (int d = 0; d < D; d++) vn += (vi[d] - pj->vel[d]) * (dr[d] / r);
+    if (vn <= 0.0) return;
+    double imp = half1pe * vn;
+    for (int d = 0; d < D; d++) vi[d] -= imp * (dr[d] / r);
+}
+
+/* 3-D: partners from the (previous step's) neighbour list, 3P operators.c:371-446.
+ * 2-D: partners from all particles in index order, 2D operators.c:324-392. */
+int oracle_collision(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg)
+{
+    int n = ps->num;
+    double l0 = cfg->particle_distance;
+    double cd = cfg->collision_distance_ratio * l0;
+    double col2 = cd * cd, dt = cfg->dt;
+    double half1pe = (1.0 + cfg->restitution_coeff) * 0.5;
+    double *after = (double *)malloc(sizeof(double) * D * (size_t)(n > 0 ? n : 1));
+    if (!after) return -1;
+    for (int i = 0; i < n; i++)
+        for (int d = 0; d < D; d++) after[(size_t)i * D + d] = ps->particles[i].vel[d];
+    for (int i = 0; i < n; i++) {
+        const Particle *pi = &ps->particles[i];
+        if (pi->type != MPS_FLUID) continue;
+        double vi[D];
+        for (int d = 0; d < D; d++) vi[d] = pi->vel[d];
+#if D == 3
+        (void)0;
+        for (int k = 0; k < nl->count[i]; k++) {
+            const Particle *pj = &ps->particles[NB(nl, i, k)];
+            if (pj->type == MPS_GHOST) continue;
+            collide_with(vi, pi, pj, col2, l0, half1pe);
+        }
+#else
+        (void)nl;
+        for (int j = 0; j < n; j++) {
+            if (j == i || ps->particles[j].type == MPS_GHOST) continue;
+            collide_with(vi, pi, &ps->particles[j], col2, l0, half1pe);
+        }
+#endif
+        for (int d = 0; d < D; d++) after[(size_t)i * D + d] = vi[d];
+    }
+    for (int i = 0; i < n; i++) {
+        Particle *p = &ps->particles[i];
+        if (p->type != MPS_FLUID) continue;
+        for (int d = 0; d < D; d++) {
+            double va = after[(size_t)i * D + d];
+            double dv = va - p->vel[d];
+            p->pos[d] += dt * dv;
+            p->vel[d] = va;
+        }
+    }
+    free(after);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* Pressure Poisson equation (3P pressure_solver.c; 2D dense variant)  */
+/* ------------------------------------------------------------------ */
+
+static inline int is_unknown(const Particle *p)
+{
+    return (p->type == MPS_FLUID && !p->on_surface) || p->type == MPS_WALL;
+}
+
+/* 3P pressure_solver.c:342-362 (high-order source term) */
+static double source_hs(const ParticleSystem *ps, const NeighborList *nl, int i,
+                        double re, const SimConfig *cfg)
+{
+    const Particle *pi = &ps->particles[i];
+    double s = 0.0;
+    for (int k = 0; k < nl->count[i]; k++) {
+        const Particle *pj = &ps->particles[NB(nl, i, k)];
+        if (pj->type == MPS_DUMMY) continue;
+        double dr[D];
+        double r2 = dist2_vec(pi->pos, pj->pos, dr);
+        if (r2 < 1.0e-24) continue;
+        double r = sqrt(r2);
+        double dv = 0.0;
+        for (int d = 0; d < D; d++) dv += dr[d] * (pj->vel[d] - pi->vel[d]);
+        s += re / (r * r * r) * dv;
+    }
+    return -(cfg->density / ps->n0 / cfg->dt) * s;
+}
+
+/* 3P pressure_solver.c:381-409 (velocity divergence for ppe_type 1) */
+static double vel_divergence(const ParticleSystem *ps, const NeighborList *nl, int i,
+                             double re, const SimConfig *cfg)
+{
+    const Particle *pi = &ps->particles[i];
+    double s = 0.0;
+    for (int k = 0; k < nl->count[i]; k++) {
+        const Particle *pj = &ps->particles[NB(nl, i, k)];
+        if (pj->type == MPS_DUMMY) continue;
+        double dr[D];
+        double r2 = dist2_vec(pi->pos, pj->pos, dr);
+        if (r2 < 1.0e-24) continue;
+        double dv = 0.0;
+        for (int d = 0; d < D; d++) dv += (pj->vel[d] - pi->vel[d]) * dr[d];
+        s += dv / r2 * KW(sqrt(r2), re);
+    }
+    return (double)D / ps->n0 * s;
+}
+
+/* Right-hand side of one unknown row, 3P pressure_solver.c:328-340,524-529. */
+static double ppe_rhs(const ParticleSystem *ps, const NeighborList *nl, int i,
+                      double re, const SimConfig *cfg)
+{
+    const Particle *p = &ps->particles[i];
+    double n0 = ps->n0, dt = cfg->dt, dt2 = dt * dt;
+    if (p->type == MPS_WALL) return 0.0;
+    if (cfg->hs_mode == 1) return source_hs(ps, nl, i, re, cfg);
+    if (cfg->ppe_type == 1) {
+        double div = (p->type == MPS_FLUID) ? vel_divergence(ps, nl, i, re, cfg) : 0.0;
+        return -cfg->density / dt * div
+               + cfg->gamma_ppe * (cfg->density / dt2) * (p->n - n0) / n0;
+    }
+    return cfg->relaxation_coeff * (cfg->density / dt2) * (p->n - n0) / n0;
+}
+
+int oracle_assemble_ppe(const ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg,
+                        int *eq_idx, int *row_ptr, int *col_idx, double *val, double *b,
+                        long long *nnz_out)
+{
+    int n = ps->num;
+    double re = cfg->influence_radius_lap;
+    double coeff = 2.0 * D / (ps->n0 * ps->lambda);
+    int n_eq = 0;
+    /* 3P pressure_solver.c:411-422: unknowns numbered in particle order. */
+    for (int i = 0; i < n; i++) eq_idx[i] = is_unknown(&ps->particles[i]) ? n_eq++ : -1;
+
+    long long nnz = 0;
+    for (int i = 0; i < n; i++) {
+        if (eq_idx[i] < 0) continue;
+        nnz += 1;
+        for (int k = 0; k < nl->count[i]; k++) {
+            int j = NB(nl, i, k);
+            if (ps->particles[j].type == MPS_DUMMY) continue;
+            if (eq_idx[j] >= 0) nnz++;
+        }
+    }
+    if (nnz_out) *nnz_out = nnz;
+    if (!row_ptr) return n_eq;
+
+    /* 3P pressure_solver.c:437-530: off-diagonals in list order, diagonal
+     * last, then the per-row insertion sort of :536-551. */
+    long long pos = 0;
+    row_ptr[0] = 0;
+    for (int i = 0; i < n; i++) {
+        int e = eq_idx[i];
+        if (e < 0) continue;
+        const Particle *pi = &ps->particles[i];
+        long long lo = pos;
+        double sum_w = 0.0;
+        for (int k = 0; k < nl->count[i]; k++) {
+            int j = NB(nl, i, k);
+            const Particle *pj = &ps->particles[j];
+            if (pj->type == MPS_DUMMY) continue;
+            double w = KW(sqrt(dist2(pi->pos, pj->pos)), re);
+            sum_w += w;
+            if (eq_idx[j] >= 0) { col_idx[pos] = eq_idx[j]; val[pos] = -coeff * w; pos++; }
+        }
+        double dv = (cfg->ppe_type == 1) ? cfg->c_ppe * coeff * sum_w : coeff * sum_w;
+        col_idx[pos] = e; val[pos] = dv; pos++;
+        for (long long p = lo + 1; p < pos; p++) {
+            int c = col_idx[p];
+            double v = val[p];
+            long long q = p - 1;
+            while (q >= lo && col_idx[q] > c) { col_idx[q + 1] = col_idx[q]; val[q + 1] = val[q]; q--; }
+            col_idx[q + 1] = c; val[q + 1] = v;
+        }
+        row_ptr[e + 1] = (int)pos;
+        b[e] = ppe_rhs(ps, nl, i, re, cfg);
+    }
+    return n_eq;
+}
+
+/* Sequential dot product, 3P pressure_solver.c:79-84. */
+static double vdot(const double *a, const double *b, int n)
+{
+    double s = 0.0;
+    for (int i = 0; i < n; i++) s += a[i] * b[i];
+    return s;
+}
+
+typedef struct { int n; const int *rp; const int *ci; const double *v; } Csr;
+
+static void csr_apply(const Csr *A, const double *x, double *y)
+{
+    for (int i = 0; i < A->n; i++) {
+        double s = 0.0;
+        for (int p = A->rp[i]; p < A->rp[i + 1]; p++) s += A->v[p] * x[A->ci[p]];
+        y[i] = s;
+    }
+}
+
+/* 3P pressure_solver.c:90-131 */
+static int cg_sparse(const Csr *A, double *x, const double *b, int maxit, double tol)
+{
+    int n = A->n;
+    double *r = malloc(sizeof(double) * n), *p = malloc(sizeof(double) * n),
+           *Ap = malloc(sizeof(double) * n);
+    if (!r || !p || !Ap) { free(r); free(p); free(Ap); return 0; }
+    memset(x, 0, sizeof(double) * n);
+    memcpy(r, b, sizeof(double) * n);
+    memcpy(p, r, sizeof(double) * n);
+    double rr = vdot(r, r, n);
+    int it;
+    for (it = 0; it < maxit; it++) {
+        if (sqrt(rr) < tol) break;
+        csr_apply(A, p, Ap);
+        double pAp = vdot(p, Ap, n);
+        if (fabs(pAp) < 1.0e-30) break;
+        double alpha = rr / pAp;
+        for (int i = 0; i < n; i++) { x[i] += alpha * p[i]; r[i] -= alpha * Ap[i]; }
+        double rr_new = vdot(r, r, n);
+        if (rr < 1.0e-60) break;
+        double beta = rr_new / rr;
+        for (int i = 0; i < n; i++) p[i] = r[i] + beta * p[i];
+        rr = rr_new;
+    }
+    g_last_resid = sqrt(rr);
+    free(r); free(p); free(Ap);
+    return it;
+}
+
+/* IC(0) on the strictly-lower pattern of A, 3P pressure_solver.c:156-232. */
+typedef struct { int n; int *rp; int *ci; double *v; double *dinv; } Lfac;
+
+static void lfac_free(Lfac *L)
+{
+    free(L->rp); free(L->ci); free(L->v); free(L->dinv);
+}
+
+static int ic0_factor(const Csr *A, const double *diag, Lfac *L)
+{
+    int n = A->n;
+    long long m = 0;
+    for (int i = 0; i < n; i++)
+        for (int p = A->rp[i]; p < A->rp[i + 1]; p++) if (A->ci[p] < i) m++;
+    L->n = n;
+    L->rp = malloc(sizeof(int) * (size_t)(n + 1));
+    L->ci = malloc(sizeof(int) * (size_t)(m + 1));
+    L->v = calloc((size_t)(m + 1), sizeof(double));
+    L->dinv = malloc(sizeof(double) * (size_t)n);
+    if (!L->rp || !L->ci || !L->v || !L->dinv) { lfac_free(L); return -1; }
+    L->rp[0] = 0;
+    for (int i = 0; i < n; i++) {
+        int q = L->rp[i];
+        for (int p = A->rp[i]; p < A->rp[i + 1]; p++)
+            if (A->ci[p] < i) { L->ci[q] = A->ci[p]; L->v[q] = A->v[p]; q++; }
+        L->rp[i + 1] = q;
+    }
+    for (int k = 0; k < n; k++) {
+        double d = diag[k];
+        for (int p = L->rp[k]; p < L->rp[k + 1]; p++) d -= L->v[p] * L->v[p];
+        if (d <= 0.0) d = (diag[k] > 0.0) ? diag[k] : 1.0e-30;
+        L->dinv[k] = 1.0 / sqrt(d);
+        for (int pk = A->rp[k]; pk < A->rp[k + 1]; pk++) {
+            int i = A->ci[pk];
+            if (i <= k) continue;
+            double s = A->v[pk];
+            int a = L->rp[i], ae = L->rp[i + 1], c = L->rp[k], ce = L->rp[k + 1];
+            while (a < ae && c < ce) {
+                int ja = L->ci[a], jc = L->ci[c];
+                if (ja < jc) a++;
+                else if (ja > jc) c++;
+                else { s -= L->v[a] * L->v[c]; a++; c++; }
+            }
+            for (int p = L->rp[i]; p < L->rp[i + 1] && L->ci[p] <= k; p++)
+                if (L->ci[p] == k) { L->v[p] = s * L->dinv[k]; break; }
+        }
+    }
+    return 0;
+}
+
+/* Forward L y = r and backward L^T z = y (scatter form), 3P :235-255. */
+static void ic0_apply(const Lfac *L, const double *r, double *tmp, double *z)
+{
+    int n = L->n;
+    for (int i = 0; i < n; i++) {
+        double s = r[i];
+        for (int p = L->rp[i]; p < L->rp[i + 1]; p++) s -= L->v[p] * tmp[L->ci[p]];
+        tmp[i] = s * L->dinv[i];
+    }
+    for (int i = 0; i < n; i++) z[i] = tmp[i];
+    for (int i = n - 1; i >= 0; i--) {
+        z[i] *= L->dinv[i];
+        for (int p = L->rp[i]; p < L->rp[i + 1]; p++) z[L->ci[p]] -= L->v[p] * z[i];
+    }
+}
+
+/* 3P pressure_solver.c:261-322; note the breakdown guard tests the OLD rz. */
+static int iccg_sparse(const Csr *A, const double *diag, double *x, const double *b,
+                       int maxit, double tol)
+{
+    int n = A->n;
+    Lfac L;
+    if (ic0_factor(A, diag, &L) != 0) return cg_sparse(A, x, b, maxit, tol);
+    double *r = malloc(sizeof(double) * n), *z = malloc(sizeof(double) * n),
+           *p = malloc(sizeof(double) * n), *Ap = malloc(sizeof(double) * n),
+           *t = malloc(sizeof(double) * n);
+    if (!r || !z || !p || !Ap || !t) {
+        free(r); free(z); free(p); free(Ap); free(t); lfac_free(&L);
+        return cg_sparse(A, x, b, maxit, tol);
+    }
+    memset(x, 0, sizeof(double) * n);
+    memcpy(r, b, sizeof(double) * n);
+    ic0_apply(&L, r, t, z);
+    memcpy(p, z, sizeof(double) * n);
+    double rz = vdot(r, z, n);
+    double rn = 0.0;
+    int it;
+    for (it = 0; it < maxit; it++) {
+        rn = sqrt(vdot(r, r, n));
+        if (rn < tol) break;
+        csr_apply(A, p, Ap);
+        double pAp = vdot(p, Ap, n);
+        if (fabs(pAp) < 1.0e-30) break;
+        double alpha = rz / pAp;
+        for (int i = 0; i < n; i++) { x[i] += alpha * p[i]; r[i] -= alpha * Ap[i]; }
+        ic0_apply(&L, r, t, z);
+        double rz_new = vdot(r, z, n);
+        if (fabs(rz) < 1.0e-60) break;
+        double beta = rz_new / rz;
+        for (int i = 0; i < n; i++) p[i] = z[i] + beta * p[i];
+        rz = rz_new;
+    }
+    g_last_resid = rn;
+    free(r); free(z); free(p); free(Ap); free(t); lfac_free(&L);
+    return it;
+}
+
+#if D == 2
+/* Dense PPE solver of the 2-D variant, 2D pressure_solver.c:35-219.  The
+ * factor keeps IC(0)'s pattern through the |A| > 0 tests and uses
+ * division by L_kk rather than a stored inverse. */
+static void dense_matvec(const double *A, const double *x, double *y, int n)
+{
+    for (int i = 0; i < n; i++) {
+        double s = 0.0;
+        const double *a = A + (size_t)i * n;
+        for (int j = 0; j < n; j++) s += a[j] * x[j];
+        y[i] = s;
+    }
+}
+
+static int dense_cg(const double *A, double *x, const double *b, int n, int maxit, double tol)
+{
+    double *r = malloc(sizeof(double) * n), *p = malloc(sizeof(double) * n),
+           *Ap = malloc(sizeof(double) * n);
+    if (!r || !p || !Ap) { free(r); free(p); free(Ap); return 0; }
+    memset(x, 0, sizeof(double) * n);
+    memcpy(r, b, sizeof(double) * n);
+    memcpy(p, r, sizeof(double) * n);
+    double rr = vdot(r, r, n);
+    int it;
+    for (it = 0; it < maxit; it++) {
+        if (sqrt(rr) < tol) break;
+        dense_matvec(A, p, Ap, n);
+        double pAp = vdot(p, Ap, n);
+        if (fabs(pAp) < 1.0e-30) break;
+        double alpha = rr / pAp;
+        for (int i = 0; i < n; i++) { x[i] += alpha * p[i]; r[i] -= alpha * Ap[i]; }
+        double rr_new = vdot(r, r, n);
+        if (rr < 1.0e-60) break;
+        double beta = rr_new / rr;
+        for (int i = 0; i < n; i++) p[i] = r[i] + beta * p[i];
+        rr = rr_new;
+    }
+    g_last_resid = sqrt(rr);
+    free(r); free(p); free(Ap);
+    return it;
+}
+
+static void dense_ic(const double *A, double *L, int n)
+{
+    memset(L, 0, sizeof(double) * (size_t)n * n);
+    for (int k = 0; k < n; k++) {
+        const double *ak = A + (size_t)k * n;
+        double *lk = L + (size_t)k * n;
+        double s = 0.0;
+        for (int j = 0; j < k; j++) if (fabs(ak[j]) > 0.0) s += lk[j] * lk[j];
+        double dg = ak[k] - s;
+        if (dg <= 0.0) dg = ak[k] > 0.0 ? ak[k] : 1.0e-30;
+        lk[k] = sqrt(dg);
+        double inv = 1.0 / lk[k];
+        for (int i = k + 1; i < n; i++) {
+            const double *ai = A + (size_t)i * n;
+            if (fabs(ai[k]) < 1.0e-30) continue;
+            double *li = L + (size_t)i * n;
+            double t = 0.0;
+            for (int j = 0; j < k; j++)
+                if (fabs(ai[j]) > 0.0 && fabs(ak[j]) > 0.0) t += li[j] * lk[j];
+            li[k] = (ai[k] - t) * inv;
+        }
+    }
+}
+
+static void dense_precond(const double *L, const double *r, double *z, double *w, int n)
+{
+    for (int i = 0; i < n; i++) {
+        const double *li = L + (size_t)i * n;
+        double s = 0.0;
+        for (int j = 0; j < i; j++) s += li[j] * w[j];
+        w[i] = (r[i] - s) / li[i];
+    }
+    for (int i = n - 1; i >= 0; i--) {
+        double s = 0.0;
+        for (int j = i + 1; j < n; j++) s += L[(size_t)j * n + i] * z[j];
+        z[i] = (w[i] - s) / L[(size_t)i * n + i];
+    }
+}
+
+static int dense_iccg(const double *A, double *x, const double *b, int n, int maxit, double tol)
+{
+    double *L = calloc((size_t)n * n, sizeof(double));
+    double *r = malloc(sizeof(double) * n), *z = malloc(sizeof(double) * n),
+           *p = malloc(sizeof(double) * n), *Ap = malloc(sizeof(double) * n),
+           *w = malloc(sizeof(double) * n);
+    if (!L || !r || !z || !p || !Ap || !w) {
+        free(L); free(r); free(z); free(p); free(Ap); free(w);
+        memset(x, 0, sizeof(double) * n);
+        return 0;
+    }
+    dense_ic(A, L, n);
+    memset(x, 0, sizeof(double) * n);
+    memcpy(r, b, sizeof(double) * n);
+    dense_precond(L, r, z, w, n);
+    memcpy(p, z, sizeof(double) * n);
+    double rz = vdot(r, z, n), rn = 0.0;
+    int it;
+    for (it = 0; it < maxit; it++) {
+        rn = sqrt(vdot(r, r, n));
+        if (rn < tol) break;
+        dense_matvec(A, p, Ap, n);
+        double pAp = vdot(p, Ap, n);
+        if (fabs(pAp) < 1.0e-30) break;
+        double alpha = rz / pAp;
+        for (int i = 0; i < n; i++) { x[i] += alpha * p[i]; r[i] -= alpha * Ap[i]; }
+        dense_precond(L, r, z, w, n);
+        double rz_new = vdot(r, z, n);
+        if (fabs(rz) < 1.0e-60) break;
+        double beta = rz_new / rz;
+        for (int i = 0; i < n; i++) p[i] = z[i] + beta * p[i];
+        rz = rz_new;
+    }
+    g_last_resid = rn;
+    free(L); free(r); free(z); free(p); free(Ap); free(w);
+    return it;
+}
+#endif
+
+int oracle_solve_pressure(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg)
+{
+    int n = ps->num;
+    int *eq = malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    if (!eq) return -1;
+    long long nnz = 0;
+    int n_eq = oracle_assemble_ppe(ps, nl, cfg, eq, NULL, NULL, NULL, NULL, &nnz);
+    g_last_iters = 0;
+    g_last_resid = 0.0;
+    if (n_eq == 0) {
+        for (int i = 0; i < n; i++) ps->particles[i].pressure = 0.0;
+        free(eq);
+        return 0;
+    }
+    int *rp = malloc(sizeof(int) * (size_t)(n_eq + 1));
+    int *ci = malloc(sizeof(int) * (size_t)nnz);
+    double *v = malloc(sizeof(double) * (size_t)nnz);
+    double *b = calloc((size_t)n_eq, sizeof(double));
+    double *x = calloc((size_t)n_eq, sizeof(double));
+    double *dg = calloc((size_t)n_eq, sizeof(double));
+    if (!rp || !ci || !v || !b || !x || !dg) {
+        free(eq); free(rp); free(ci); free(v); free(b); free(x); free(dg);
+        return -1;
+    }
+    oracle_assemble_ppe(ps, nl, cfg, eq, rp, ci, v, b, NULL);
+    for (int e = 0; e < n_eq; e++)
+        for (int p = rp[e]; p < rp[e + 1]; p++) if (ci[p] == e) dg[e] = v[p];
+
+    int it;
+#if D == 3
+    Csr A = {n_eq, rp, ci, v};
+    it = (cfg->solver_type == 1) ? iccg_sparse(&A, dg, x, b, cfg->cg_max_iter, cfg->cg_tolerance)
+                                 : cg_sparse(&A, x, b, cfg->cg_max_iter, cfg->cg_tolerance);
+#else
+    /* The 2-D reference builds a dense n_eq x n_eq matrix (2D :346). */
+    double *M = calloc((size_t)n_eq * n_eq, sizeof(double));
+    if (!M) {
+        free(eq); free(rp); free(ci); free(v); free(b); free(x); free(dg);
+        return -1;
+    }
+    for (int e = 0; e < n_eq; e++)
+        for (int p = rp[e]; p < rp[e + 1]; p++) M[(size_t)e * n_eq + ci[p]] = v[p];
+    it = (cfg->solver_type == 1) ? dense_iccg(M, x, b, n_eq, cfg->cg_max_iter, cfg->cg_tolerance)
+                                 : dense_cg(M, x, b, n_eq, cfg->cg_max_iter, cfg->cg_tolerance);
+    free(M);
+#endif
+    g_last_iters = it;
+    for (int i = 0; i < n; i++) ps->particles[i].pressure = (eq[i] >= 0) ? x[eq[i]] : 0.0;
+    free(eq); free(rp); free(ci); free(v); free(b); free(x); free(dg);
+    return it;
+}
+
+/* ------------------------------------------------------------------ */
+/* Boundary bookkeeping (3P boundary.c:12-61)                          */
+/* ------------------------------------------------------------------ */
+
+void oracle_apply_wall_boundary(ParticleSystem *ps)
+{
+    for (int i = 0; i < ps->num; i++) {
+        Particle *p = &ps->particles[i];
+        if (p->type == MPS_WALL || p->type == MPS_GHOST)
+            for (int d = 0; d < D; d++) { p->vel[d] = 0.0; p->acc[d] = 0.0; }
+    }
+}
+
+void oracle_remove_out_of_bounds(ParticleSystem *ps, const SimConfig *cfg)
+{
+    double m = cfg->particle_distance * (cfg->wall_layers + 1);
+    for (int i = 0; i < ps->num; i++) {
+        Particle *p = &ps->particles[i];
+        if (p->type != MPS_FLUID) continue;
+        int out = 0;
+        for (int d = 0; d < D; d++) {
+            double x = p->pos[d];
+            if (x < cfg->domain_min[d] - m || x > cfg->domain_max[d] + m || isnan(x)) out = 1;
+        }
+        if (out) {
+            p->type = MPS_GHOST;
+            p->pressure = 0.0;
+            p->n = 0.0;
+            for (int d = 0; d < D; d++) { p->vel[d] = 0.0; p->acc[d] = 0.0; }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* One time step (3P simulation.c:19-118; 2D simulation.c:25-118)      */
+/* ------------------------------------------------------------------ */
+
+int oracle_step(ParticleSystem *ps, NeighborList *nl, CellList *cl, const SimConfig *cfg)
+{
+    double re = fmax(cfg->influence_radius_lap, cfg->influence_radius_n);
+    if (cfg->surface_tension_enabled) return -2;   /* outside the restated path */
+    double dt = cfg->dt;
+    int n = ps->num;
+
+    for (int i = 0; i < n; i++) {
+        Particle *p = &ps->particles[i];
+        for (int d = 0; d < D; d++) p->acc[d] = (p->type == MPS_FLUID) ? cfg->gravity[d] : 0.0;
+    }
+    oracle_viscosity(ps, nl, cfg);
+    for (int i = 0; i < n; i++) {
+        Particle *p = &ps->particles[i];
+        if (p->type != MPS_FLUID) continue;
+        for (int d = 0; d < D; d++) p->vel[d] += dt * p->acc[d];
+    }
+    for (int i = 0; i < n; i++) {
+        Particle *p = &ps->particles[i];
+        if (p->type != MPS_FLUID) continue;
+        for (int d = 0; d < D; d++) p->pos[d] += dt * p->vel[d];
+    }
+#if D == 3
+    if (cfg->collision_distance_ratio > 0.0)
+#endif
+        if (oracle_collision(ps, nl, cfg) != 0) return -1;
+
+    int rc = oracle_neighbor_search(nl, ps, cl, re);
+    if (rc != 0) return rc;
+    oracle_number_density(ps, nl, cfg);
+    if (cfg->surface_detection_method == 1) {
+        oracle_neighbor_count(ps, nl, cfg);
+        oracle_judge_free_surface_by_count(ps, cfg->surface_count_threshold);
+    } else {
+        oracle_judge_free_surface(ps, cfg->surface_threshold);
+    }
+    if (oracle_solve_pressure(ps, nl, cfg) < 0) return -1;
+    if (cfg->clamp_negative_pressure) oracle_clamp_pressure(ps);
+    if (oracle_pressure_gradient(ps, nl, cfg) != 0) return -1;
+    for (int i = 0; i < n; i++) {
+        Particle *p = &ps->particles[i];
+        if (p->type != MPS_FLUID) continue;
+        for (int d = 0; d < D; d++) {
+            double du = dt * p->acc[d];
+            p->vel[d] += du;
+            p->pos[d] += dt * du;
+        }
+    }
+    oracle_apply_wall_boundary(ps);
+    oracle_remove_out_of_bounds(ps, cfg);
+    return 0;
+}
