@@ -1,0 +1,188 @@
+/*
+ * mps_b200.h -- C ABI of the B200 (sm_100a) MPS time-step library.
+ *
+ * Two layers, both plain C (pointers, sizes, status codes; no torch types):
+ *
+ *  1. The session API below (mps_*).  A session owns one device-resident
+ *     particle system on the current CUDA device and runs the whole time
+ *     step there.  It takes a dimension-independent parameter struct.
+ *
+ *  2. The drop-in API (include/mps_dropin.h): the reference solver's own
+ *     function names and structs, implemented over the session API and built
+ *     per dimension into libmps3d.so / libmps2d.so.
+ *
+ * Every entry point returns MPS_OK (0) or a negative MPS_ERR_* code; the
+ * reference's exit(1) / silent-return failure modes become codes here.
+ */
+#ifndef MPS_B200_H
+#define MPS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPS_OK                      0
+#define MPS_ERR_INVALID           (-1)  /* bad argument or state */
+#define MPS_ERR_CUDA              (-2)  /* a CUDA call failed */
+#define MPS_ERR_OOM               (-3)  /* device allocation failed */
+#define MPS_ERR_NEIGHBOR_OVERFLOW (-4)  /* a particle has more than max_neighbors
+                                           (reference: neighbor_search.c:221-228 exit) */
+#define MPS_ERR_UNSUPPORTED       (-5)  /* switch outside the implemented path */
+#define MPS_ERR_NOT_CONVERGED     (-6)  /* reported, never raised by default */
+#define MPS_ERR_NAN               (-7)
+
+/* Precision forms of the step. */
+#define MPS_PREC_FP64  0   /* the reference's arithmetic, FP64 everywhere */
+#define MPS_PREC_MIXED 1   /* FP32 operators/SpMV/IC(0), FP64 dots, refinement, integration */
+
+/* PPE unknown orderings for the IC(0) preconditioner. */
+#define MPS_ORDER_BLOCK_COLOR 0  /* cells as blocks, 2^dim colours (default) */
+
+/* Simulation parameters, the hot-path subset of the reference SimConfig
+ * (mps_fluid3D_parallel/include/sim_config.h:10-78) with radii already
+ * derived (re = ratio * l0) and fixed 3-element vectors for both dims. */
+typedef struct {
+    int    dim;                       /* 2 or 3 */
+    double particle_distance;         /* l0 */
+    double influence_radius_lap;
+    double influence_radius_n;
+    int    max_neighbors;
+    int    wall_layers;
+    double density;
+    double viscosity;
+    double gravity[3];
+    double dt;
+    int    solver_type;               /* 0: CG, 1: ICCG */
+    int    cg_max_iter;
+    double cg_tolerance;
+    double relaxation_coeff;
+    int    clamp_negative_pressure;
+    int    ppe_type;
+    double c_ppe;
+    double gamma_ppe;
+    double surface_threshold;
+    int    surface_detection_method;
+    double surface_count_threshold;
+    double restitution_coeff;
+    double collision_distance_ratio;
+    int    surface_tension_enabled;   /* must be 0: not on this path */
+    double domain_min[3];
+    double domain_max[3];
+    int    cmps_gradient;
+    int    use_analytical_lambda;
+    int    hs_mode;
+    int    precision;                 /* MPS_PREC_* */
+    double refine_tolerance;          /* mixed form: inner FP32 relative tolerance */
+} mps_params_t;
+
+/* Per-step metrics (the reference computes and discards its iteration count,
+ * pressure_solver.c:553-561). */
+typedef struct {
+    int    ppe_iterations;            /* CG iterations of the last step (inner, summed) */
+    int    ppe_outer;                 /* refinement sweeps (mixed form), else 1 */
+    double ppe_residual;              /* final recursive residual norm */
+    int    n_eq;
+    long long nnz;
+    int    n_fluid;
+    int    n_ghost;
+    int    converged;
+    long long total_iterations;       /* over the session */
+    long long total_steps;
+    double ms_ops;                    /* device time of the last step outside the PPE */
+    double ms_assembly;
+    double ms_factor;
+    double ms_solve;
+} mps_metrics_t;
+
+typedef struct mps_session mps_session;
+
+int  mps_version(void);
+const char *mps_error_string(int code);
+
+/* Lifetime.  Creates device buffers for up to `capacity` particles on the
+ * current CUDA device (cudaSetDevice beforehand picks the GPU). */
+int  mps_session_create(mps_session **out, const mps_params_t *params, int capacity);
+int  mps_session_destroy(mps_session *s);
+/* Replace the parameters (a changed domain or radius rebuilds the grid and
+ * requires a new neighbour search). */
+int  mps_update_params(mps_session *s, const mps_params_t *params);
+/* Human-readable detail of the session's last failure. */
+const char *mps_last_error(mps_session *s);
+
+/* State transfer in the reference's particle order.  `particles` points at
+ * `num` AoS Particle records of the session's dimension (104 bytes each in
+ * 3-D, 80 in 2-D; include/mps_types.h).  Upload replaces the state; download
+ * writes pos, vel, acc, pressure, n, neighbor_count, type and on_surface. */
+int  mps_upload_particles(mps_session *s, const void *particles, int num);
+int  mps_download_particles(mps_session *s, void *particles, int num);
+/* SoA transfer of positions/velocities/types only (host arrays of num*dim
+ * doubles, particle-major). */
+int  mps_upload_soa(mps_session *s, const double *pos, const double *vel, const int *type, int num);
+int  mps_download_pressure(mps_session *s, double *pressure, int num);
+
+/* Reference quantities n0, lambda, N0.  compute: on the device, with the
+ * reference's rule (particle.c:69-221: first strictly largest n0_i in index
+ * order, sums in ascending j).  set: take them from the caller. */
+int  mps_compute_initial_params(mps_session *s, double *n0, double *lambda, int *n0_count);
+int  mps_set_initial_params(mps_session *s, double n0, double lambda, int n0_count);
+
+/* Neighbour search at the current positions (the step's cell sort).  Must run
+ * once after an upload and before the first step, as simulation_run does. */
+int  mps_neighbor_search(mps_session *s);
+
+/* `nsteps` full time steps, device-resident (simulation.c:19-118). */
+int  mps_step(mps_session *s, int nsteps);
+
+/* One full step whose explicit stage (viscosity, 3-D collision) uses the
+ * caller's neighbour list from the previous step, as the reference's
+ * simulation_step(ps, nl, cl, step) does; the state comes from the last
+ * upload.  Afterwards the session holds the fresh structure. */
+int  mps_step_with_list(mps_session *s, const int *neighbors, const int *count, int max_nb);
+
+/* Neighbour sets of the current structure in the reference's layout: for
+ * each particle i (reference order) count[i] entries neighbors[i*max_nb+k]
+ * in the reference's list order.  Either pointer may be NULL. */
+int  mps_get_neighbor_list(mps_session *s, int *neighbors, int *count, int max_nb);
+/* Cell index of each particle (reference order) as the reference computes
+ * it, -1 for ghosts and particles outside the grid. */
+int  mps_get_cell_index(mps_session *s, int *cell);
+/* The reference's CellList chains of the current structure: head[total_cells]
+ * (first = largest index of each cell, -1 if empty) and next[num]. */
+int  mps_get_cell_links(mps_session *s, int *head, int *next, int total_cells);
+
+/* PPE of the current state in the reference's unknown numbering (particle
+ * order): eq_idx[num], row_ptr[n_eq+1], col_idx/val[nnz] (sorted columns,
+ * diagonal included), b[n_eq].  Call with row_ptr == NULL to get sizes. */
+int  mps_get_ppe(mps_session *s, int *eq_idx, int *row_ptr, int *col_idx, double *val,
+                 double *b, int *n_eq, long long *nnz);
+
+int  mps_get_metrics(mps_session *s, mps_metrics_t *m);
+
+/* The stream all session work is issued on (a cudaStream_t). */
+void *mps_get_stream(mps_session *s);
+
+/* Stage entry points over a caller-supplied neighbour list (the reference's
+ * NeighborList layout; host pointers).  The state is taken from the last
+ * upload in reference order; results are read back with download.  These
+ * back the drop-in's fine-grained functions. */
+#define MPS_STAGE_DENSITY        1   /* calc_particle_number_density  (operators.c:17) */
+#define MPS_STAGE_VISCOSITY      2   /* calc_viscosity_term           (operators.c:50) */
+#define MPS_STAGE_GRADIENT       3   /* calc_pressure_gradient        (operators.c:102) */
+#define MPS_STAGE_NEIGHBOR_COUNT 4   /* calc_neighbor_count           (operators.c:226) */
+#define MPS_STAGE_COLLISION      5   /* collision                     (operators.c:371) */
+#define MPS_STAGE_SOLVE_PRESSURE 6   /* solve_pressure                (pressure_solver.c:368) */
+#define MPS_STAGE_SURFACE        7   /* judge_free_surface[_by_count] (operators.c:206,253) */
+#define MPS_STAGE_CLAMP          8   /* clamp_pressure                (operators.c:188) */
+#define MPS_STAGE_WALL           9   /* apply_wall_boundary           (boundary.c:12) */
+#define MPS_STAGE_OUT_OF_BOUNDS 10   /* remove_out_of_bounds          (boundary.c:33) */
+int  mps_run_stage(mps_session *s, int stage, const int *neighbors, const int *count,
+                   int max_nb, double arg);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MPS_B200_H */

@@ -1,0 +1,1273 @@
+// engine.cu -- the device-resident MPS time step on sm_100a and its C ABI.
+//
+// One Engine<D> owns a particle system in HBM as structure-of-arrays, kept
+// sorted by (cell, descending reference index) and re-sorted at every
+// neighbour search.  A step is (mps_fluid3D_parallel/src/simulation.c:19-118):
+//
+//   viscosity + gravity        k_viscosity       previous step's structure
+//   explicit u*, r*            k_explicit_update
+//   collision                  k_collision_*     previous structure (3-D) or
+//                                                a fresh sort (2-D all-pairs)
+//   neighbour search           sort()            counting sort by cell
+//   number density + surface   k_density
+//   PPE                        ppe()             assembly, IC(0), PCG
+//   clamp (optional)           k_writeback
+//   pressure gradient          k_pmin, k_gradient
+//   correction, wall, ghosts   k_correct
+//
+// All work is issued on one stream; the host synchronises twice per step
+// to size the PPE (n_eq, nnz) and once per CG batch to test convergence.
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <numeric>
+
+#include "engine.cuh"
+#include "k_ops.cuh"
+#include "k_ppe.cuh"
+#include "k_sort.cuh"
+
+namespace mps {
+
+static inline int nblk(long long n, int b) { return (int)((n + b - 1) / b); }
+
+constexpr int TPB = 256;             // threads per block, particle kernels
+constexpr int RED_BLOCKS = 148 * 4;  // fixed grid of the reduction kernels
+constexpr int CG_BATCH = 8;          // CG iterations between convergence reads
+
+template <int D>
+struct AosLayout {
+    static constexpr int size = (24 * D + 28 + 7) / 8 * 8;   // 104 (3-D), 80 (2-D)
+    static constexpr int pos = 0, vel = 8 * D, acc = 16 * D, pressure = 24 * D, n = 24 * D + 8,
+                         ncount = 24 * D + 16, type = 24 * D + 20, surf = 24 * D + 24;
+};
+
+template <int D>
+__global__ void k_unpack(const unsigned char *__restrict__ aos, State<D> s, int num)
+{
+    using L = AosLayout<D>;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= num) return;
+    const unsigned char *r = aos + (size_t)i * L::size;
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+        double x = *(const double *)(r + L::pos + 8 * d);
+        s.pos[d][i] = x;
+        s.key[d][i] = x;
+        s.vel[d][i] = *(const double *)(r + L::vel + 8 * d);
+        s.acc[d][i] = *(const double *)(r + L::acc + 8 * d);
+    }
+    s.p[i] = *(const double *)(r + L::pressure);
+    s.n[i] = *(const double *)(r + L::n);
+    s.ncount[i] = *(const int *)(r + L::ncount);
+    s.type[i] = *(const int *)(r + L::type);
+    s.surf[i] = *(const int *)(r + L::surf);
+    s.id[i] = i;
+    s.cell[i] = -1;
+}
+
+template <int D>
+__global__ void k_pack(unsigned char *__restrict__ aos, State<D> s, int num)
+{
+    using L = AosLayout<D>;
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= num) return;
+    unsigned char *r = aos + (size_t)s.id[q] * L::size;
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+        *(double *)(r + L::pos + 8 * d) = s.pos[d][q];
+        *(double *)(r + L::vel + 8 * d) = s.vel[d][q];
+        *(double *)(r + L::acc + 8 * d) = s.acc[d][q];
+    }
+    *(double *)(r + L::pressure) = s.p[q];
+    *(double *)(r + L::n) = s.n[q];
+    *(int *)(r + L::ncount) = s.ncount[q];
+    *(int *)(r + L::type) = s.type[q];
+    *(int *)(r + L::surf) = s.surf[q];
+    *(int *)(r + L::surf + 4) = 0;
+}
+
+template <int D>
+__global__ void k_unpack_soa(const double *__restrict__ pos, const double *__restrict__ vel,
+                             const int *__restrict__ type, State<D> s, int num)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= num) return;
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+        double x = pos[(size_t)i * D + d];
+        s.pos[d][i] = x;
+        s.key[d][i] = x;
+        s.vel[d][i] = vel[(size_t)i * D + d];
+        s.acc[d][i] = 0.0;
+    }
+    s.p[i] = 0.0;
+    s.n[i] = 0.0;
+    s.ncount[i] = 0;
+    s.type[i] = type[i];
+    s.surf[i] = 0;
+    s.id[i] = i;
+    s.cell[i] = -1;
+}
+
+template <int D>
+__global__ void k_pressure_ref(State<D> s, int num, double *__restrict__ out)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < num) out[s.id[q]] = s.p[q];
+}
+
+__global__ void k_cell_links(const int *__restrict__ start, const int *__restrict__ id, const int *__restrict__ cell,
+                             int total, int n, int *__restrict__ head, int *__restrict__ next)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < total) {
+        int b = start[q], e = start[q + 1];
+        head[q] = (b < e) ? id[b] : -1;
+    }
+    if (q < n) {
+        int c = cell[q];
+        int nx = -1;
+        if (c >= 0 && q + 1 < start[c + 1]) nx = id[q + 1];
+        next[id[q]] = nx;
+    }
+}
+
+// CSR rows in the reference's numbering (for parity checks): row of
+// reference particle i = eq[i]; columns renumbered, then sorted by the host.
+__global__ void k_ppe_to_ref(int n_eq, const int *__restrict__ part_of_row, const int *__restrict__ id,
+                             const int *__restrict__ eq_by_id, const int *__restrict__ row_ptr,
+                             const int *__restrict__ col, const double *__restrict__ val,
+                             const double *__restrict__ b, const int *__restrict__ part_of_col_row,
+                             const int *__restrict__ ref_row_ptr, int *__restrict__ out_col,
+                             double *__restrict__ out_val, double *__restrict__ out_b)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_eq) return;
+    int i = id[part_of_row[r]];
+    int er = eq_by_id[i];
+    int o = ref_row_ptr[er];
+    for (int q = row_ptr[r]; q < row_ptr[r + 1]; q++) {
+        out_col[o] = eq_by_id[id[part_of_col_row[col[q]]]];
+        out_val[o] = val[q];
+        o++;
+    }
+    out_b[er] = b[r];
+}
+
+template <int D>
+class Engine final : public EngineBase {
+public:
+    Engine(const mps_params_t &p, int capacity);
+    ~Engine() override;
+    int dim() const override { return D; }
+    void update_params(const mps_params_t &p) override;
+    void upload_aos(const void *aos, int num) override;
+    void download_aos(void *aos, int num) override;
+    void upload_soa(const double *pos, const double *vel, const int *type, int num) override;
+    void download_pressure(double *p, int num) override;
+    void compute_initial_params(double *n0, double *lambda, int *n0_count) override;
+    void set_initial_params(double n0, double lambda, int n0_count) override;
+    void neighbor_search() override;
+    void step(int nsteps) override;
+    void step_with_list(const int *nb, const int *cnt, int max_nb) override;
+    void get_neighbor_list(int *nb, int *cnt, int max_nb) override;
+    void get_cell_index(int *cell) override;
+    void get_cell_links(int *head, int *next, int total) override;
+    void get_ppe(int *eq_idx, int *row_ptr, int *col, double *val, double *b, int *n_eq,
+                 long long *nnz) override;
+    void run_stage(int stage, const int *nb, const int *cnt, int max_nb, double arg) override;
+    cudaStream_t stream() const override { return st_; }
+
+private:
+    // ---- configuration
+    mps_params_t prm_{};
+    Consts k_{};
+    Grid<D> g_{};
+    double re_list_ = 0.0;
+    double n0_ = 0.0, lambda_ = 0.0;
+    int n0_count_ = 0;
+    bool have_ref_ = false;
+    int cap_ = 0, n_ = 0;
+    cudaStream_t st_ = nullptr;
+
+    // ---- particle state, double-buffered across sorts
+    DevArray<double> dbuf_[2];
+    DevArray<int> ibuf_[2];
+    State<D> S_[2];
+    int cur_ = 0;
+    bool structure_ = false;   // cell structure valid for S_[cur_]
+
+    // ---- sort
+    DevArray<int> kcell_, count_, start_, cursor_, excl_, exoff_, tmp_, perm_, where_, scanws_;
+    DevArray<long long> scanws64_;
+
+    // ---- block colouring
+    DevArray<int> ccells_;
+    std::vector<int> color_off_;
+
+    // ---- PPE
+    DevArray<int> ucount_, ucol_, rs_, cell_row0_, row_of_, part_of_row_, rcount_, row_ptr_, diagpos_, col_;
+    DevArray<double> A_, F_, b_, x_, r_, z_, p_, Ap_, y_, partials_;
+    DevArray<CGScalars> sc_;
+    DevArray<unsigned> ticket_, err_;
+    int n_eq_ = 0;
+    long long nnz_ = 0;
+    bool ppe_valid_ = false;
+
+    // ---- misc
+    DevArray<double> vafter_, pmin_;
+    DevArray<int> lptr_, lidx_, lout_, lcnt_;
+    DevArray<unsigned char> aos_;
+    DevArray<double> soa_in_;
+    DevArray<int> int_in_;
+    CGScalars *sc_host_ = nullptr;
+    int *int_host_ = nullptr;
+    cudaEvent_t ev_[6];
+
+    State<D> &S() { return S_[cur_]; }
+    CellSource<D> cells() const
+    {
+        CellSource<D> c;
+        c.g = g_;
+        for (int d = 0; d < D; d++) c.key[d] = S_[cur_].key[d];
+        c.cell = S_[cur_].cell;
+        c.re2 = k_.re_list2;
+        return c;
+    }
+
+    void alloc_state();
+    void build_grid();
+    void compute_consts();
+    void sort();
+    void unsort();
+    void ppe(bool clamp);
+    int read_int(const int *dev);
+    void check_err();
+    void upload_list(const int *nb, const int *cnt, int max_nb);
+    ListSource list() const { return ListSource{lptr_.p, lidx_.p}; }
+    void explicit_stage(bool from_list);
+    void implicit_stage();
+    void require_ref() const
+    {
+        if (!have_ref_) throw CudaError("n0/lambda not set: call compute or set initial params", MPS_ERR_INVALID);
+    }
+};
+
+// ---------------------------------------------------------------------------
+
+template <int D>
+Engine<D>::Engine(const mps_params_t &p, int capacity)
+{
+    if (p.dim != D) throw CudaError("dimension mismatch", MPS_ERR_INVALID);
+    if (capacity <= 0) throw CudaError("capacity must be positive", MPS_ERR_INVALID);
+    if (p.surface_tension_enabled) throw CudaError("surface tension is not on this path", MPS_ERR_UNSUPPORTED);
+    cap_ = capacity;
+    prm_ = p;
+    MPS_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
+    for (auto &e : ev_) MPS_CUDA(cudaEventCreate(&e));
+    MPS_CUDA(cudaMallocHost((void **)&sc_host_, sizeof(CGScalars)));
+    MPS_CUDA(cudaMallocHost((void **)&int_host_, 16 * sizeof(int)));
+    alloc_state();
+    build_grid();
+    compute_consts();
+    sc_.reserve(1);
+    ticket_.reserve(4);
+    err_.reserve(1);
+    partials_.reserve(2 * RED_BLOCKS + 8);
+    MPS_CUDA(cudaMemsetAsync(ticket_.p, 0, 4 * sizeof(unsigned), st_));
+    MPS_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(unsigned), st_));
+
+    // Neighbour-cell visit orders for PPE rows: sorted by (colour, z, y, x).
+    signed char t3[8][27][3], t2[4][9][2];
+    for (int par = 0; par < (1 << D); par++) {
+        std::vector<std::array<int, 3>> offs;
+        for (int dz = (D == 3 ? -1 : 0); dz <= (D == 3 ? 1 : 0); dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) offs.push_back({dx, dy, dz});
+        auto color = [&](const std::array<int, 3> &o) {
+            int c = 0;
+            for (int d = 0; d < D; d++) c |= (((par >> d) & 1) ^ (o[d] & 1)) << d;
+            return c;
+        };
+        std::stable_sort(offs.begin(), offs.end(),
+                         [&](const std::array<int, 3> &a, const std::array<int, 3> &b) {
+                             return color(a) < color(b);
+                         });
+        for (size_t q = 0; q < offs.size(); q++)
+            for (int d = 0; d < D; d++) {
+                if (D == 3) t3[par][q][d] = (signed char)offs[q][d];
+                else t2[par][q][d] = (signed char)offs[q][d];
+            }
+    }
+    if (D == 3) MPS_CUDA(cudaMemcpyToSymbol(c_order3, t3, sizeof(t3)));
+    else MPS_CUDA(cudaMemcpyToSymbol(c_order2, t2, sizeof(t2)));
+}
+
+template <int D>
+Engine<D>::~Engine()
+{
+    if (st_) cudaStreamSynchronize(st_);
+    for (auto &e : ev_) cudaEventDestroy(e);
+    if (sc_host_) cudaFreeHost(sc_host_);
+    if (int_host_) cudaFreeHost(int_host_);
+    if (st_) cudaStreamDestroy(st_);
+}
+
+template <int D>
+void Engine<D>::alloc_state()
+{
+    size_t nd = (size_t)(4 * D + 2), ni = 5;
+    for (int b = 0; b < 2; b++) {
+        dbuf_[b].reserve(nd * cap_);
+        ibuf_[b].reserve(ni * cap_);
+        double *dp = dbuf_[b].p;
+        int *ip = ibuf_[b].p;
+        State<D> &s = S_[b];
+        for (int d = 0; d < D; d++) {
+            s.pos[d] = dp + (size_t)(0 * D + d) * cap_;
+            s.vel[d] = dp + (size_t)(1 * D + d) * cap_;
+            s.acc[d] = dp + (size_t)(2 * D + d) * cap_;
+            s.key[d] = dp + (size_t)(3 * D + d) * cap_;
+        }
+        s.p = dp + (size_t)(4 * D) * cap_;
+        s.n = dp + (size_t)(4 * D + 1) * cap_;
+        s.type = ip;
+        s.surf = ip + (size_t)cap_;
+        s.ncount = ip + 2 * (size_t)cap_;
+        s.id = ip + 3 * (size_t)cap_;
+        s.cell = ip + 4 * (size_t)cap_;
+    }
+    kcell_.reserve(cap_);
+    excl_.reserve(cap_);
+    exoff_.reserve(cap_ + 1);
+    tmp_.reserve(cap_);
+    perm_.reserve(cap_);
+    where_.reserve(cap_);
+    vafter_.reserve((size_t)D * cap_);
+    pmin_.reserve(cap_);
+    row_of_.reserve(cap_);
+    part_of_row_.reserve(cap_);
+    rcount_.reserve(cap_ + 1);
+    row_ptr_.reserve(cap_ + 1);
+    diagpos_.reserve(cap_);
+    for (auto *v : {&b_, &x_, &r_, &z_, &p_, &Ap_, &y_}) v->reserve(cap_);
+}
+
+// cell_list_create (neighbor_search.c:92-122) with cell size = list radius.
+template <int D>
+void Engine<D>::build_grid()
+{
+    double re = std::fmax(prm_.influence_radius_lap, prm_.influence_radius_n);
+    re_list_ = re;
+    double margin = 4.0 * re;
+    long long total = 1;
+    for (int d = 0; d < D; d++) {
+        g_.origin[d] = prm_.domain_min[d] - margin;
+        double span = (prm_.domain_max[d] + margin) - g_.origin[d];
+        g_.dims[d] = (int)(span / re) + 2;
+        total *= g_.dims[d];
+    }
+    if (total <= 0 || total > (1LL << 30)) throw CudaError("cell grid too large", MPS_ERR_INVALID);
+    g_.total = (int)total;
+    g_.cs_inv = 1.0 / re;
+    count_.reserve(total + 1);
+    cursor_.reserve(total + 1);
+    start_.reserve(total + 2);
+    ucount_.reserve(total);
+    ucol_.reserve(total);
+    rs_.reserve(total + 1);
+    cell_row0_.reserve(total);
+    size_t ws = std::max(scan_workspace((int)std::max<long long>(total + 1, cap_ + 1)), (size_t)64);
+    scanws_.reserve(ws);
+    g_.start = start_.p;
+
+    // cells sorted by (colour, linear index)
+    std::vector<int> cc((size_t)total);
+    int ncol = 1 << D;
+    std::vector<int> cnt(ncol + 1, 0);
+    auto color_of = [&](long long lin) {
+        int c = 0;
+        for (int d = 0; d < D; d++) {
+            c |= (int)((lin % g_.dims[d]) & 1) << d;
+            lin /= g_.dims[d];
+        }
+        return c;
+    };
+    for (long long l = 0; l < total; l++) cnt[color_of(l) + 1]++;
+    for (int c = 0; c < ncol; c++) cnt[c + 1] += cnt[c];
+    color_off_ = cnt;
+    std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+    for (long long l = 0; l < total; l++) cc[(size_t)fill[color_of(l)]++] = (int)l;
+    ccells_.reserve(total);
+    MPS_CUDA(cudaMemcpy(ccells_.p, cc.data(), sizeof(int) * (size_t)total, cudaMemcpyHostToDevice));
+}
+
+// Constants evaluated with the reference's expressions.
+template <int D>
+void Engine<D>::compute_consts()
+{
+    const mps_params_t &p = prm_;
+    Consts &k = k_;
+    k.l0 = p.particle_distance;
+    k.rmin = 0.01 * p.particle_distance;
+    k.re_lap = p.influence_radius_lap;
+    k.re_n = p.influence_radius_n;
+    k.re_list2 = re_list_ * re_list_;
+    k.re_n2 = p.influence_radius_n * p.influence_radius_n;
+    double n0 = have_ref_ ? n0_ : 1.0, lambda = have_ref_ ? lambda_ : 1.0;
+    k.n0 = n0;
+    k.coeff = 2.0 * D / (n0 * lambda);
+    k.visc_coeff = p.viscosity * k.coeff;
+    k.grad_coeff = (double)D / n0;
+    k.neg_grad = -k.grad_coeff;
+    k.density = p.density;
+    for (int d = 0; d < 3; d++) k.gravity[d] = d < D ? p.gravity[d] : 0.0;
+    k.dt = p.dt;
+    double cd = p.collision_distance_ratio * p.particle_distance;
+    k.col2 = cd * cd;
+    k.col_rmin = 1.0e-12 * p.particle_distance;
+    k.half1pe = (1.0 + p.restitution_coeff) * 0.5;
+    k.grad_r2min = p.particle_distance * p.particle_distance * 1.0e-12;
+    k.surf_thr = p.surface_threshold * n0;
+    k.count_thr = p.surface_count_threshold * n0_count_;
+    k.diag_scale = (p.ppe_type == 1) ? p.c_ppe * k.coeff : k.coeff;
+    k.neg_coeff = -k.coeff;
+    double dt2 = p.dt * p.dt;
+    k.rhs_k = p.relaxation_coeff * (p.density / dt2);
+    k.rhs_hs = -(p.density / n0 / p.dt);
+    k.rhs_na = -p.density / p.dt;
+    k.rhs_nb = p.gamma_ppe * (p.density / dt2);
+    double margin = p.particle_distance * (p.wall_layers + 1);
+    for (int d = 0; d < 3; d++) {
+        k.oob_lo[d] = p.domain_min[d] - margin;
+        k.oob_hi[d] = p.domain_max[d] + margin;
+    }
+    k.max_nb = p.max_neighbors;
+    k.ppe_type = p.ppe_type;
+    k.hs_mode = p.hs_mode;
+    k.cmps = p.cmps_gradient;
+    k.surf_method = p.surface_detection_method;
+    k.clamp = p.clamp_negative_pressure;
+    k.collision_on = (D == 2) ? 1 : (p.collision_distance_ratio > 0.0);
+}
+
+template <int D>
+void Engine<D>::update_params(const mps_params_t &p)
+{
+    if (p.dim != D) throw CudaError("dimension mismatch", MPS_ERR_INVALID);
+    if (p.surface_tension_enabled) throw CudaError("surface tension is not on this path", MPS_ERR_UNSUPPORTED);
+    bool regrid = false;
+    for (int d = 0; d < D; d++)
+        regrid |= p.domain_min[d] != prm_.domain_min[d] || p.domain_max[d] != prm_.domain_max[d];
+    regrid |= std::fmax(p.influence_radius_lap, p.influence_radius_n) != re_list_;
+    prm_ = p;
+    if (regrid) {
+        build_grid();
+        structure_ = false;
+    }
+    compute_consts();
+}
+
+template <int D>
+int Engine<D>::read_int(const int *dev)
+{
+    MPS_CUDA(cudaMemcpyAsync(int_host_, dev, sizeof(int), cudaMemcpyDeviceToHost, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+    return int_host_[0];
+}
+
+template <int D>
+void Engine<D>::check_err()
+{
+    unsigned e = 0;
+    MPS_CUDA(cudaMemcpyAsync(int_host_, err_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+    MPS_CUDA(cudaGetLastError());
+    std::memcpy(&e, int_host_, sizeof(unsigned));
+    if (e) {
+        MPS_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(unsigned), st_));
+        if (e & ERR_NEIGHBOR_OVERFLOW) throw CudaError("neighbour count exceeded max_neighbors", MPS_ERR_NEIGHBOR_OVERFLOW);
+        if (e & ERR_UNKNOWN_OFF_GRID) throw CudaError("a PPE unknown lies outside the cell grid", MPS_ERR_UNSUPPORTED);
+        if (e & ERR_LIST_MISMATCH) throw CudaError("neighbour list does not match the cell structure", MPS_ERR_UNSUPPORTED);
+        if (e & ERR_COLORING) throw CudaError("PPE row count mismatch", MPS_ERR_INVALID);
+        throw CudaError("device error", MPS_ERR_INVALID);
+    }
+}
+
+// ---- state transfer ---------------------------------------------------------
+
+template <int D>
+void Engine<D>::upload_aos(const void *aos, int num)
+{
+    if (num < 0 || num > cap_) throw CudaError("particle count exceeds capacity", MPS_ERR_INVALID);
+    n_ = num;
+    size_t bytes = (size_t)num * AosLayout<D>::size;
+    aos_.reserve(bytes + 8);
+    MPS_CUDA(cudaMemcpyAsync(aos_.p, aos, bytes, cudaMemcpyHostToDevice, st_));
+    if (num) k_unpack<D><<<nblk(num, TPB), TPB, 0, st_>>>(aos_.p, S(), num);
+    MPS_CUDA(cudaGetLastError());
+    MPS_CUDA(cudaStreamSynchronize(st_));
+    structure_ = false;
+    ppe_valid_ = false;
+}
+
+template <int D>
+void Engine<D>::download_aos(void *aos, int num)
+{
+    if (num != n_) throw CudaError("download count differs from the uploaded count", MPS_ERR_INVALID);
+    size_t bytes = (size_t)num * AosLayout<D>::size;
+    aos_.reserve(bytes + 8);
+    if (num) k_pack<D><<<nblk(num, TPB), TPB, 0, st_>>>(aos_.p, S(), num);
+    MPS_CUDA(cudaGetLastError());
+    MPS_CUDA(cudaMemcpyAsync(aos, aos_.p, bytes, cudaMemcpyDeviceToHost, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+}
+
+template <int D>
+void Engine<D>::upload_soa(const double *pos, const double *vel, const int *type, int num)
+{
+    if (num < 0 || num > cap_) throw CudaError("particle count exceeds capacity", MPS_ERR_INVALID);
+    n_ = num;
+    soa_in_.reserve((size_t)2 * D * num + 2);
+    int_in_.reserve((size_t)num + 1);
+    MPS_CUDA(cudaMemcpyAsync(soa_in_.p, pos, sizeof(double) * D * num, cudaMemcpyHostToDevice, st_));
+    MPS_CUDA(cudaMemcpyAsync(soa_in_.p + (size_t)D * num, vel, sizeof(double) * D * num,
+                             cudaMemcpyHostToDevice, st_));
+    MPS_CUDA(cudaMemcpyAsync(int_in_.p, type, sizeof(int) * num, cudaMemcpyHostToDevice, st_));
+    if (num)
+        k_unpack_soa<D><<<nblk(num, TPB), TPB, 0, st_>>>(soa_in_.p, soa_in_.p + (size_t)D * num, int_in_.p, S(),
+                                                         num);
+    MPS_CUDA(cudaGetLastError());
+    MPS_CUDA(cudaStreamSynchronize(st_));
+    structure_ = false;
+    ppe_valid_ = false;
+}
+
+template <int D>
+void Engine<D>::download_pressure(double *p, int num)
+{
+    if (num != n_) throw CudaError("download count differs from the uploaded count", MPS_ERR_INVALID);
+    soa_in_.reserve((size_t)num + 2);
+    if (num) k_pressure_ref<D><<<nblk(num, TPB), TPB, 0, st_>>>(S(), num, soa_in_.p);
+    MPS_CUDA(cudaMemcpyAsync(p, soa_in_.p, sizeof(double) * num, cudaMemcpyDeviceToHost, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+}
+
+// ---- neighbour search -------------------------------------------------------
+
+template <int D>
+void Engine<D>::sort()
+{
+    int n = n_, total = g_.total;
+    State<D> &src = S_[cur_];
+    State<D> &dst = S_[cur_ ^ 1];
+    MPS_CUDA(cudaMemsetAsync(count_.p, 0, sizeof(int) * (total + 1), st_));
+    MPS_CUDA(cudaMemsetAsync(cursor_.p, 0, sizeof(int) * (total + 1), st_));
+    if (n) k_bin<D><<<nblk(n, TPB), TPB, 0, st_>>>(src, g_, n, kcell_.p, count_.p, excl_.p);
+    scan_exclusive<int>(count_.p, start_.p, total, scanws_.p, st_);
+    scan_exclusive<int>(excl_.p, exoff_.p, n, scanws_.p, st_);
+    if (n) {
+        k_scatter<<<nblk(n, TPB), TPB, 0, st_>>>(n, total, kcell_.p, start_.p, cursor_.p, exoff_.p, tmp_.p,
+                                                 perm_.p);
+        // ranks for the binned prefix [0, start[total])
+        k_rank<<<nblk(n, TPB), TPB, 0, st_>>>(start_.p + total, tmp_.p, kcell_.p, start_.p, src.id, perm_.p);
+        k_gather<D><<<nblk(n, TPB), TPB, 0, st_>>>(dst, src, perm_.p, kcell_.p, n, where_.p);
+    }
+    MPS_CUDA(cudaGetLastError());
+    cur_ ^= 1;
+    g_.start = start_.p;
+    structure_ = true;
+    ppe_valid_ = false;
+}
+
+template <int D>
+void Engine<D>::unsort()
+{
+    int n = n_;
+    if (n) k_unsort<D><<<nblk(n, TPB), TPB, 0, st_>>>(S_[cur_ ^ 1], S_[cur_], where_.p, n);
+    MPS_CUDA(cudaGetLastError());
+    cur_ ^= 1;
+    structure_ = false;
+    ppe_valid_ = false;
+}
+
+template <int D>
+void Engine<D>::neighbor_search()
+{
+    sort();
+    if (n_) {
+        // list lengths only: the reference aborts on overflow during the search
+        lcnt_.reserve((size_t)n_ + 1);
+        k_build_list<D><<<nblk(n_, TPB), TPB, 0, st_>>>(cells(), S().id, n_, k_.max_nb, nullptr, lcnt_.p, err_.p);
+    }
+    check_err();
+}
+
+// ---- initial parameters (f1) -----------------------------------------------
+
+template <int D>
+void Engine<D>::compute_initial_params(double *n0, double *lambda, int *n0_count)
+{
+    int n = n_;
+    if (n == 0) throw CudaError("no particles", MPS_ERR_INVALID);
+    // bounding box on the host side of a copy of the positions
+    std::vector<double> h((size_t)n * D);
+    for (int d = 0; d < D; d++)
+        MPS_CUDA(cudaMemcpyAsync(h.data() + (size_t)d * n, S().pos[d], sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                 st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+    double lo[D], hi[D];
+    for (int d = 0; d < D; d++) {
+        lo[d] = INFINITY;
+        hi[d] = -INFINITY;
+        for (int i = 0; i < n; i++) {
+            double v = h[(size_t)d * n + i];
+            lo[d] = std::min(lo[d], v);
+            hi[d] = std::max(hi[d], v);
+        }
+        if (!std::isfinite(lo[d]) || !std::isfinite(hi[d]))
+            throw CudaError("non-finite particle position", MPS_ERR_NAN);
+    }
+    double re_n = prm_.influence_radius_n, re_lap = prm_.influence_radius_lap;
+    double rmax = std::max(re_n, re_lap);
+    double cs = rmax * (1.0 + 1.0e-9);
+    Grid<D> bg{};
+    long long total = 1;
+    for (int d = 0; d < D; d++) {
+        bg.origin[d] = lo[d];
+        bg.dims[d] = (int)((hi[d] - lo[d]) / cs) + 1;
+        total *= bg.dims[d];
+    }
+    if (total > (1LL << 30)) throw CudaError("bounding-box grid too large", MPS_ERR_INVALID);
+    bg.total = (int)total;
+    DevArray<int> gcell, cnt, st, cur, order, cnti, qbest;
+    DevArray<double> dlo, n0i, numi, deni, best;
+    gcell.reserve(n);
+    cnt.reserve(total + 1);
+    st.reserve(total + 2);
+    cur.reserve(total + 1);
+    order.reserve(n);
+    cnti.reserve(n);
+    qbest.reserve(4);
+    dlo.reserve(D);
+    n0i.reserve(n);
+    numi.reserve(n);
+    deni.reserve(n);
+    best.reserve(2);
+    DevArray<int> ws;
+    ws.reserve(scan_workspace((int)total + 1) + 8);
+    MPS_CUDA(cudaMemcpyAsync(dlo.p, lo, sizeof(double) * D, cudaMemcpyHostToDevice, st_));
+    MPS_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * (total + 1), st_));
+    MPS_CUDA(cudaMemsetAsync(cur.p, 0, sizeof(int) * (total + 1), st_));
+    k_bbox_cell<D><<<nblk(n, TPB), TPB, 0, st_>>>(S(), n, bg, cs, dlo.p, gcell.p, cnt.p);
+    scan_exclusive<int>(cnt.p, st.p, (int)total, ws.p, st_);
+    k_bbox_scatter<<<nblk(n, TPB), TPB, 0, st_>>>(n, gcell.p, st.p, cur.p, order.p);
+    bg.start = st.p;
+    k_initial_params<D><<<nblk(n, 128), 128, 0, st_>>>(S(), n, bg, gcell.p, order.p, rmax, re_n, re_lap,
+                                                       0.01 * prm_.particle_distance, n0i.p, numi.p, deni.p,
+                                                       cnti.p, err_.p);
+    k_initial_argmax<D><<<1, 1024, 0, st_>>>(S(), n, n0i.p, cnti.p, best.p, qbest.p, qbest.p + 1);
+    MPS_CUDA(cudaGetLastError());
+    check_err();
+    double bv;
+    int q[2];
+    MPS_CUDA(cudaMemcpy(&bv, best.p, sizeof(double), cudaMemcpyDeviceToHost));
+    MPS_CUDA(cudaMemcpy(q, qbest.p, 2 * sizeof(int), cudaMemcpyDeviceToHost));
+    double num = 0.0, den = 0.0;
+    if (bv > 0.0 && q[0] >= 0) {
+        MPS_CUDA(cudaMemcpy(&num, numi.p + q[0], sizeof(double), cudaMemcpyDeviceToHost));
+        MPS_CUDA(cudaMemcpy(&den, deni.p + q[0], sizeof(double), cudaMemcpyDeviceToHost));
+        n0_ = bv;
+        if (prm_.use_analytical_lambda)
+            lambda_ = re_lap * re_lap * (double)D * (double)(D - 1) / ((double)(D + 1) * (double)(D + 2));
+        else
+            lambda_ = (den > 1.0e-10) ? num / den : 1.0;
+        if (prm_.surface_detection_method == 1) n0_count_ = q[1];
+    } else {
+        // particle.c:159-164: no fluid particle with a positive n0
+        n0_ = 1.0;
+        lambda_ = 1.0;
+    }
+    have_ref_ = true;
+    compute_consts();
+    if (n0) *n0 = n0_;
+    if (lambda) *lambda = lambda_;
+    if (n0_count) *n0_count = n0_count_;
+}
+
+template <int D>
+void Engine<D>::set_initial_params(double n0, double lambda, int n0_count)
+{
+    n0_ = n0;
+    lambda_ = lambda;
+    n0_count_ = n0_count;
+    have_ref_ = true;
+    compute_consts();
+}
+
+// ---- the step -------------------------------------------------------------------
+
+template <int D>
+void Engine<D>::upload_list(const int *nb, const int *cnt, int max_nb)
+{
+    int n = n_;
+    std::vector<int> ptr((size_t)n + 1, 0);
+    for (int i = 0; i < n; i++) {
+        if (cnt[i] < 0 || cnt[i] > max_nb) throw CudaError("bad neighbour count", MPS_ERR_INVALID);
+        ptr[i + 1] = ptr[i] + cnt[i];
+    }
+    std::vector<int> idx((size_t)ptr[n] + 1);
+    for (int i = 0; i < n; i++) {
+        const int *row = nb + (size_t)i * max_nb;
+        for (int k = 0; k < cnt[i]; k++) {
+            int j = row[k];
+            if (j < 0 || j >= n) throw CudaError("neighbour index out of range", MPS_ERR_INVALID);
+            idx[(size_t)ptr[i] + k] = j;
+        }
+    }
+    lptr_.reserve((size_t)n + 1);
+    lidx_.reserve(idx.size());
+    MPS_CUDA(cudaMemcpyAsync(lptr_.p, ptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st_));
+    MPS_CUDA(cudaMemcpyAsync(lidx_.p, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+}
+
+template <int D>
+void Engine<D>::explicit_stage(bool from_list)
+{
+    int n = n_;
+    if (!n) return;
+    int nb = nblk(n, TPB);
+    if (from_list) k_viscosity<D, ListSource><<<nb, TPB, 0, st_>>>(list(), S(), k_, n, 0);
+    else k_viscosity<D, CellSource<D>><<<nb, TPB, 0, st_>>>(cells(), S(), k_, n, 0);
+    k_explicit_update<D><<<nb, TPB, 0, st_>>>(S(), k_, n);
+    if (k_.collision_on) {
+        if (D == 3) {
+            if (from_list) k_collision_list<D, ListSource><<<nb, TPB, 0, st_>>>(list(), S(), k_, n, vafter_.p);
+            else k_collision_list<D, CellSource<D>><<<nb, TPB, 0, st_>>>(cells(), S(), k_, n, vafter_.p);
+        } else {
+            sort();
+            k_collision_allpairs<D><<<nb, TPB, 0, st_>>>(cells(), S(), k_, n, vafter_.p);
+        }
+        k_collision_apply<D><<<nb, TPB, 0, st_>>>(S(), k_, n, vafter_.p);
+    }
+    MPS_CUDA(cudaGetLastError());
+}
+
+template <int D>
+void Engine<D>::implicit_stage()
+{
+    int n = n_;
+    sort();
+    if (!n) return;
+    int nb = nblk(n, TPB);
+    k_density<D, CellSource<D>><<<nb, TPB, 0, st_>>>(cells(), S(), k_, n, err_.p, 1, 1);
+    MPS_CUDA(cudaEventRecord(ev_[1], st_));
+    ppe(k_.clamp != 0);
+    MPS_CUDA(cudaEventRecord(ev_[4], st_));
+    if (k_.cmps != 2) k_pmin<D, CellSource<D>><<<nb, TPB, 0, st_>>>(cells(), S(), n, pmin_.p);
+    k_gradient<D, CellSource<D>><<<nb, TPB, 0, st_>>>(cells(), S(), k_, n, k_.cmps != 2 ? pmin_.p : nullptr);
+    k_correct<D><<<nb, TPB, 0, st_>>>(S(), k_, n, 1, 1, 1);
+    MPS_CUDA(cudaGetLastError());
+}
+
+template <int D>
+void Engine<D>::step(int nsteps)
+{
+    require_ref();
+    if (!structure_) throw CudaError("no neighbour structure: run the neighbour search first", MPS_ERR_INVALID);
+    for (int s = 0; s < nsteps; s++) {
+        MPS_CUDA(cudaEventRecord(ev_[0], st_));
+        explicit_stage(false);
+        implicit_stage();
+        MPS_CUDA(cudaEventRecord(ev_[5], st_));
+        check_err();
+        float t01 = 0, t12 = 0, t23 = 0, t34 = 0, t45 = 0;
+        cudaEventElapsedTime(&t01, ev_[0], ev_[1]);
+        cudaEventElapsedTime(&t12, ev_[1], ev_[2]);
+        cudaEventElapsedTime(&t23, ev_[2], ev_[3]);
+        cudaEventElapsedTime(&t34, ev_[3], ev_[4]);
+        cudaEventElapsedTime(&t45, ev_[4], ev_[5]);
+        met.ms_ops = t01 + t45;
+        met.ms_assembly = t12;
+        met.ms_factor = t23;
+        met.ms_solve = t34;
+        met.total_steps++;
+    }
+}
+
+template <int D>
+void Engine<D>::step_with_list(const int *nb, const int *cnt, int max_nb)
+{
+    require_ref();
+    if (structure_) unsort();
+    upload_list(nb, cnt, max_nb);
+    MPS_CUDA(cudaEventRecord(ev_[0], st_));
+    explicit_stage(true);
+    implicit_stage();
+    MPS_CUDA(cudaEventRecord(ev_[5], st_));
+    check_err();
+    met.total_steps++;
+}
+
+// ---- PPE ------------------------------------------------------------------------
+
+template <int D>
+void Engine<D>::ppe(bool clamp)
+{
+    int n = n_, total = g_.total;
+    int ncol = 1 << D;
+    State<D> &s = S();
+    k_cell_unknowns<D><<<nblk(total, TPB), TPB, 0, st_>>>(s, start_.p, total, ucount_.p);
+    k_color_gather<<<nblk(total, TPB), TPB, 0, st_>>>(ccells_.p, ucount_.p, total, ucol_.p);
+    scan_exclusive<int>(ucol_.p, rs_.p, total, scanws_.p, st_);
+    k_assign_rows<D><<<nblk(total, TPB), TPB, 0, st_>>>(s, start_.p, ccells_.p, rs_.p, total, cell_row0_.p,
+                                                        row_of_.p, part_of_row_.p);
+    int nbinned = read_int(start_.p + total);
+    if (n > nbinned) k_offgrid_rows<D><<<nblk(n - nbinned, TPB), TPB, 0, st_>>>(s, nbinned, n, row_of_.p, err_.p);
+    int n_eq = read_int(rs_.p + total);
+    n_eq_ = n_eq;
+    met.n_eq = n_eq;
+    int nb = nblk(n, TPB);
+    if (n_eq == 0) {
+        met.ppe_iterations = 0;
+        met.ppe_residual = 0.0;
+        met.converged = 1;
+        met.nnz = 0;
+        MPS_CUDA(cudaEventRecord(ev_[2], st_));
+        MPS_CUDA(cudaEventRecord(ev_[3], st_));
+        k_writeback<D><<<nb, TPB, 0, st_>>>(s, row_of_.p, x_.p, n, clamp);
+        ppe_valid_ = true;
+        return;
+    }
+    CellSource<D> src = cells();
+    k_row_count<D, CellSource<D>><<<nblk(n_eq, TPB), TPB, 0, st_>>>(src, s, part_of_row_.p, row_of_.p, n_eq,
+                                                                     rcount_.p);
+    scan_exclusive<int>(rcount_.p, row_ptr_.p, n_eq, scanws_.p, st_);
+    int nnz = read_int(row_ptr_.p + n_eq);
+    if (nnz < 0) throw CudaError("PPE too large for 32-bit row pointers", MPS_ERR_UNSUPPORTED);
+    nnz_ = nnz;
+    met.nnz = nnz;
+    col_.reserve(nnz);
+    A_.reserve(nnz);
+    F_.reserve(nnz);
+    k_fill<D><<<nblk(n_eq, 128), 128, 0, st_>>>(src, s, k_, part_of_row_.p, row_of_.p, n_eq, row_ptr_.p, col_.p,
+                                                A_.p, diagpos_.p, b_.p, err_.p);
+    MPS_CUDA(cudaEventRecord(ev_[2], st_));
+    bool icc = prm_.solver_type == 1;
+    if (icc) {
+        MPS_CUDA(cudaMemcpyAsync(F_.p, A_.p, sizeof(double) * nnz, cudaMemcpyDeviceToDevice, st_));
+        for (int c = 0; c < ncol; c++) {
+            int kb = color_off_[c], ke = color_off_[c + 1];
+            if (ke > kb)
+                k_ic0_color<<<nblk((long long)(ke - kb) * 32, 256), 256, 0, st_>>>(
+                    kb, ke, ccells_.p, cell_row0_.p, ucount_.p, row_ptr_.p, diagpos_.p, col_.p, A_.p, F_.p);
+        }
+    }
+    MPS_CUDA(cudaEventRecord(ev_[3], st_));
+
+    // PCG (pressure_solver.c:261-322); CG when solver_type == 0 (:90-131).
+    CGScalars init{};
+    init.tol = prm_.cg_tolerance;
+    init.maxit = prm_.cg_max_iter;
+    MPS_CUDA(cudaMemcpyAsync(sc_.p, &init, sizeof(CGScalars), cudaMemcpyHostToDevice, st_));
+    const int RB = RED_BLOCKS;
+    k_cg_init<<<RB, CG_BLOCK, 0, st_>>>(n_eq, x_.p, r_.p, b_.p);
+    double *z = icc ? z_.p : r_.p;
+    auto precond = [&]() {
+        for (int c = 0; c < ncol; c++) {
+            int kb = color_off_[c], ke = color_off_[c + 1];
+            if (ke > kb)
+                k_fwd_color<<<nblk((long long)(ke - kb) * 32, 256), 256, 0, st_>>>(
+                    kb, ke, ccells_.p, cell_row0_.p, ucount_.p, row_ptr_.p, diagpos_.p, col_.p, F_.p, r_.p, y_.p,
+                    sc_.p);
+        }
+        for (int c = ncol - 1; c >= 0; c--) {
+            int kb = color_off_[c], ke = color_off_[c + 1];
+            if (ke > kb)
+                k_bwd_color<<<nblk((long long)(ke - kb) * 32, 256), 256, 0, st_>>>(
+                    kb, ke, ccells_.p, cell_row0_.p, ucount_.p, row_ptr_.p, diagpos_.p, col_.p, F_.p, y_.p, z_.p,
+                    sc_.p);
+        }
+    };
+    if (icc) precond();
+    k_cg_init2<<<RB, CG_BLOCK, 0, st_>>>(n_eq, r_.p, z, p_.p, partials_.p, ticket_.p, sc_.p);
+    for (;;) {
+        for (int it = 0; it < CG_BATCH; it++) {
+            k_cg_spmv<32><<<RB, CG_BLOCK, 0, st_>>>(n_eq, row_ptr_.p, col_.p, A_.p, p_.p, Ap_.p, partials_.p,
+                                                   ticket_.p, sc_.p);
+            k_cg_axpy<<<RB, CG_BLOCK, 0, st_>>>(n_eq, x_.p, r_.p, p_.p, Ap_.p, partials_.p, ticket_.p, sc_.p);
+            if (icc) precond();
+            k_cg_rz<<<RB, CG_BLOCK, 0, st_>>>(n_eq, r_.p, z, partials_.p, ticket_.p, sc_.p);
+            k_cg_update_p<<<RB, CG_BLOCK, 0, st_>>>(n_eq, p_.p, z, sc_.p);
+        }
+        MPS_CUDA(cudaGetLastError());
+        MPS_CUDA(cudaMemcpyAsync(sc_host_, sc_.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, st_));
+        MPS_CUDA(cudaStreamSynchronize(st_));
+        if (sc_host_->done) break;
+    }
+    met.ppe_iterations = sc_host_->iter;
+    met.ppe_outer = 1;
+    met.ppe_residual = std::sqrt(sc_host_->rr);
+    met.converged = std::sqrt(sc_host_->rr) < prm_.cg_tolerance;
+    met.total_iterations += sc_host_->iter;
+    k_writeback<D><<<nb, TPB, 0, st_>>>(s, row_of_.p, x_.p, n, clamp);
+    MPS_CUDA(cudaGetLastError());
+    ppe_valid_ = true;
+}
+
+// ---- introspection --------------------------------------------------------
+
+template <int D>
+void Engine<D>::get_neighbor_list(int *nb, int *cnt, int max_nb)
+{
+    if (!structure_) throw CudaError("no neighbour structure", MPS_ERR_INVALID);
+    int n = n_;
+    if (max_nb <= 0) throw CudaError("max_nb must be positive", MPS_ERR_INVALID);
+    size_t slots = (size_t)n * max_nb;
+    if (nb) lout_.reserve(slots + 1);
+    lcnt_.reserve((size_t)n + 1);
+    if (n)
+        k_build_list<D><<<nblk(n, TPB), TPB, 0, st_>>>(cells(), S().id, n, max_nb, nb ? lout_.p : nullptr,
+                                                       lcnt_.p, err_.p);
+    MPS_CUDA(cudaGetLastError());
+    if (nb) MPS_CUDA(cudaMemcpyAsync(nb, lout_.p, sizeof(int) * slots, cudaMemcpyDeviceToHost, st_));
+    if (cnt) MPS_CUDA(cudaMemcpyAsync(cnt, lcnt_.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st_));
+    check_err();
+}
+
+template <int D>
+void Engine<D>::get_cell_index(int *cell)
+{
+    if (!structure_) throw CudaError("no neighbour structure", MPS_ERR_INVALID);
+    int n = n_;
+    lcnt_.reserve((size_t)n + 1);
+    if (n) k_cell_ref_order<D><<<nblk(n, TPB), TPB, 0, st_>>>(S().cell, S().id, n, lcnt_.p);
+    MPS_CUDA(cudaMemcpyAsync(cell, lcnt_.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+}
+
+template <int D>
+void Engine<D>::get_cell_links(int *head, int *next, int total)
+{
+    if (!structure_) throw CudaError("no neighbour structure", MPS_ERR_INVALID);
+    if (total != g_.total) throw CudaError("cell count differs from the session grid", MPS_ERR_INVALID);
+    int n = n_;
+    DevArray<int> h, nx;
+    h.reserve(total + 1);
+    nx.reserve((size_t)n + 1);
+    int m = std::max(total, n);
+    if (m) k_cell_links<<<nblk(m, TPB), TPB, 0, st_>>>(start_.p, S().id, S().cell, total, n, h.p, nx.p);
+    if (head) MPS_CUDA(cudaMemcpyAsync(head, h.p, sizeof(int) * total, cudaMemcpyDeviceToHost, st_));
+    if (next) MPS_CUDA(cudaMemcpyAsync(next, nx.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+}
+
+template <int D>
+void Engine<D>::get_ppe(int *eq_idx, int *row_ptr, int *col, double *val, double *b, int *n_eq, long long *nnz)
+{
+    if (!ppe_valid_) throw CudaError("no assembled PPE: run a step or the solve stage first", MPS_ERR_INVALID);
+    if (n_eq) *n_eq = n_eq_;
+    if (nnz) *nnz = nnz_;
+    if (!row_ptr) return;
+    int n = n_, ne = n_eq_;
+    // reference numbering: unknowns in reference index order
+    DevArray<int> by_id, eq_by_id, rp_ref, ccol;
+    DevArray<double> cval, cb;
+    by_id.reserve(n + 1);
+    eq_by_id.reserve(n + 1);
+    if (n) k_ref_eq<<<nblk(n, TPB), TPB, 0, st_>>>(row_of_.p, S().id, n, by_id.p);
+    std::vector<int> h_by(n), h_eq(n);
+    MPS_CUDA(cudaMemcpyAsync(h_by.data(), by_id.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st_));
+    std::vector<int> h_rp(ne + 1);
+    MPS_CUDA(cudaMemcpyAsync(h_rp.data(), row_ptr_.p, sizeof(int) * (ne + 1), cudaMemcpyDeviceToHost, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+    int e = 0;
+    std::vector<int> eng_row_of_ref(ne);
+    for (int i = 0; i < n; i++) {
+        if (h_by[i] >= 0) { eng_row_of_ref[e] = h_by[i]; h_eq[i] = e++; }
+        else h_eq[i] = -1;
+    }
+    std::vector<int> ref_rp(ne + 1, 0);
+    for (int r = 0; r < ne; r++) ref_rp[r + 1] = ref_rp[r] + (h_rp[eng_row_of_ref[r] + 1] - h_rp[eng_row_of_ref[r]]);
+    MPS_CUDA(cudaMemcpyAsync(eq_by_id.p, h_eq.data(), sizeof(int) * n, cudaMemcpyHostToDevice, st_));
+    rp_ref.reserve(ne + 1);
+    MPS_CUDA(cudaMemcpyAsync(rp_ref.p, ref_rp.data(), sizeof(int) * (ne + 1), cudaMemcpyHostToDevice, st_));
+    ccol.reserve(nnz_ + 1);
+    cval.reserve(nnz_ + 1);
+    cb.reserve(ne + 1);
+    if (ne)
+        k_ppe_to_ref<<<nblk(ne, TPB), TPB, 0, st_>>>(ne, part_of_row_.p, S().id, eq_by_id.p, row_ptr_.p, col_.p,
+                                                      A_.p, b_.p, part_of_row_.p, rp_ref.p, ccol.p, cval.p, cb.p);
+    std::vector<int> hc(nnz_);
+    std::vector<double> hv(nnz_);
+    MPS_CUDA(cudaMemcpyAsync(hc.data(), ccol.p, sizeof(int) * nnz_, cudaMemcpyDeviceToHost, st_));
+    MPS_CUDA(cudaMemcpyAsync(hv.data(), cval.p, sizeof(double) * nnz_, cudaMemcpyDeviceToHost, st_));
+    if (b) MPS_CUDA(cudaMemcpyAsync(b, cb.p, sizeof(double) * ne, cudaMemcpyDeviceToHost, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+    // sort each row by column (the reference's insertion sort, :536-551)
+    std::vector<std::pair<int, double>> rowbuf;
+    for (int r = 0; r < ne; r++) {
+        rowbuf.clear();
+        for (int q = ref_rp[r]; q < ref_rp[r + 1]; q++) rowbuf.push_back({hc[q], hv[q]});
+        std::sort(rowbuf.begin(), rowbuf.end(),
+                  [](const std::pair<int, double> &a, const std::pair<int, double> &b2) { return a.first < b2.first; });
+        for (int q = ref_rp[r]; q < ref_rp[r + 1]; q++) {
+            if (col) col[q] = rowbuf[q - ref_rp[r]].first;
+            if (val) val[q] = rowbuf[q - ref_rp[r]].second;
+        }
+    }
+    std::memcpy(row_ptr, ref_rp.data(), sizeof(int) * (ne + 1));
+    if (eq_idx) std::memcpy(eq_idx, h_eq.data(), sizeof(int) * n);
+}
+
+// ---- stages over a caller list (drop-in fine-grained functions) ----------------
+
+template <int D>
+void Engine<D>::run_stage(int stage, const int *nb, const int *cnt, int max_nb, double arg)
+{
+    int n = n_;
+    bool needs_list = stage == MPS_STAGE_DENSITY || stage == MPS_STAGE_VISCOSITY || stage == MPS_STAGE_GRADIENT ||
+                      stage == MPS_STAGE_NEIGHBOR_COUNT || stage == MPS_STAGE_SOLVE_PRESSURE ||
+                      (stage == MPS_STAGE_COLLISION && D == 3);
+    bool needs_ref = stage == MPS_STAGE_VISCOSITY || stage == MPS_STAGE_GRADIENT ||
+                     stage == MPS_STAGE_SOLVE_PRESSURE || stage == MPS_STAGE_SURFACE;
+    if (needs_ref) require_ref();
+    if (needs_list && (!nb || !cnt)) throw CudaError("stage needs a neighbour list", MPS_ERR_INVALID);
+    if (structure_ && stage != MPS_STAGE_CLAMP && stage != MPS_STAGE_WALL && stage != MPS_STAGE_OUT_OF_BOUNDS &&
+        stage != MPS_STAGE_SURFACE)
+        unsort();
+    if (needs_list) upload_list(nb, cnt, max_nb);
+    int bl = nblk(n, TPB);
+    if (n == 0) return;
+    switch (stage) {
+    case MPS_STAGE_DENSITY:
+        k_density<D, ListSource><<<bl, TPB, 0, st_>>>(list(), S(), k_, n, err_.p, 0, 0);
+        break;
+    case MPS_STAGE_VISCOSITY:
+        k_viscosity<D, ListSource><<<bl, TPB, 0, st_>>>(list(), S(), k_, n, 1);
+        break;
+    case MPS_STAGE_GRADIENT:
+        if (k_.cmps != 2) k_pmin<D, ListSource><<<bl, TPB, 0, st_>>>(list(), S(), n, pmin_.p);
+        k_gradient<D, ListSource><<<bl, TPB, 0, st_>>>(list(), S(), k_, n, k_.cmps != 2 ? pmin_.p : nullptr);
+        break;
+    case MPS_STAGE_NEIGHBOR_COUNT:
+        k_neighbor_count<D, ListSource><<<bl, TPB, 0, st_>>>(list(), S(), k_, n);
+        break;
+    case MPS_STAGE_COLLISION:
+        if (D == 3) {
+            k_collision_list<D, ListSource><<<bl, TPB, 0, st_>>>(list(), S(), k_, n, vafter_.p);
+        } else {
+            sort();
+            k_collision_allpairs<D><<<bl, TPB, 0, st_>>>(cells(), S(), k_, n, vafter_.p);
+        }
+        k_collision_apply<D><<<bl, TPB, 0, st_>>>(S(), k_, n, vafter_.p);
+        break;
+    case MPS_STAGE_SOLVE_PRESSURE: {
+        // the block-colour solver needs the cell structure; the caller's
+        // list must be the one that structure produces
+        sort();
+        k_compare_list<D><<<bl, TPB, 0, st_>>>(cells(), S().id, n, lptr_.p, lidx_.p, err_.p);
+        check_err();
+        ppe(false);
+        break;
+    }
+    case MPS_STAGE_SURFACE: {
+        Consts k = k_;
+        int by_count = prm_.surface_detection_method == 1;
+        if (by_count) k.count_thr = arg * n0_count_;
+        else k.surf_thr = arg * n0_;
+        k_surface<D><<<bl, TPB, 0, st_>>>(S(), k, n, by_count);
+        break;
+    }
+    case MPS_STAGE_CLAMP:
+        k_clamp<D><<<bl, TPB, 0, st_>>>(S(), n);
+        break;
+    case MPS_STAGE_WALL:
+        k_correct<D><<<bl, TPB, 0, st_>>>(S(), k_, n, 0, 1, 0);
+        break;
+    case MPS_STAGE_OUT_OF_BOUNDS:
+        k_correct<D><<<bl, TPB, 0, st_>>>(S(), k_, n, 0, 0, 1);
+        break;
+    default:
+        throw CudaError("unknown stage", MPS_ERR_INVALID);
+    }
+    MPS_CUDA(cudaGetLastError());
+    check_err();
+}
+
+EngineBase *make_engine(const mps_params_t &p, int capacity)
+{
+    if (p.dim == 3) return new Engine<3>(p, capacity);
+    if (p.dim == 2) return new Engine<2>(p, capacity);
+    throw CudaError("dim must be 2 or 3", MPS_ERR_INVALID);
+}
+
+}  // namespace mps
+
+// =============================================================================
+// C ABI
+// =============================================================================
+
+struct mps_session {
+    std::unique_ptr<mps::EngineBase> eng;
+};
+
+#define MPS_API_BODY(s, body)                                          \
+    do {                                                               \
+        if (!(s) || !(s)->eng) return MPS_ERR_INVALID;                 \
+        try {                                                          \
+            body;                                                      \
+            return MPS_OK;                                             \
+        } catch (const mps::CudaError &e) {                            \
+            (s)->eng->last_error = e.what();                           \
+            return e.code;                                             \
+        } catch (const std::bad_alloc &) {                             \
+            return MPS_ERR_OOM;                                        \
+        } catch (const std::exception &e) {                            \
+            (s)->eng->last_error = e.what();                           \
+            return MPS_ERR_INVALID;                                    \
+        }                                                              \
+    } while (0)
+
+extern "C" {
+
+int mps_version(void) { return 10000; }
+
+const char *mps_error_string(int code)
+{
+    switch (code) {
+    case MPS_OK: return "ok";
+    case MPS_ERR_INVALID: return "invalid argument or state";
+    case MPS_ERR_CUDA: return "CUDA error";
+    case MPS_ERR_OOM: return "out of device memory";
+    case MPS_ERR_NEIGHBOR_OVERFLOW: return "neighbour count exceeded max_neighbors";
+    case MPS_ERR_UNSUPPORTED: return "unsupported configuration";
+    case MPS_ERR_NOT_CONVERGED: return "PPE solve did not converge";
+    case MPS_ERR_NAN: return "non-finite value";
+    default: return "unknown error";
+    }
+}
+
+int mps_session_create(mps_session **out, const mps_params_t *params, int capacity)
+{
+    if (!out || !params) return MPS_ERR_INVALID;
+    *out = nullptr;
+    try {
+        auto *s = new mps_session;
+        s->eng.reset(mps::make_engine(*params, capacity));
+        *out = s;
+        return MPS_OK;
+    } catch (const mps::CudaError &e) {
+        std::fprintf(stderr, "mps_session_create: %s\n", e.what());
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        return MPS_ERR_OOM;
+    }
+}
+
+int mps_session_destroy(mps_session *s)
+{
+    delete s;
+    return MPS_OK;
+}
+
+int mps_update_params(mps_session *s, const mps_params_t *p)
+{
+    if (!p) return MPS_ERR_INVALID;
+    MPS_API_BODY(s, s->eng->update_params(*p));
+}
+
+int mps_upload_particles(mps_session *s, const void *particles, int num)
+{
+    if (!particles && num) return MPS_ERR_INVALID;
+    MPS_API_BODY(s, s->eng->upload_aos(particles, num));
+}
+
+int mps_download_particles(mps_session *s, void *particles, int num)
+{
+    if (!particles && num) return MPS_ERR_INVALID;
+    MPS_API_BODY(s, s->eng->download_aos(particles, num));
+}
+
+int mps_upload_soa(mps_session *s, const double *pos, const double *vel, const int *type, int num)
+{
+    if ((!pos || !vel || !type) && num) return MPS_ERR_INVALID;
+    MPS_API_BODY(s, s->eng->upload_soa(pos, vel, type, num));
+}
+
+int mps_download_pressure(mps_session *s, double *pressure, int num)
+{
+    if (!pressure && num) return MPS_ERR_INVALID;
+    MPS_API_BODY(s, s->eng->download_pressure(pressure, num));
+}
+
+int mps_compute_initial_params(mps_session *s, double *n0, double *lambda, int *n0_count)
+{
+    MPS_API_BODY(s, s->eng->compute_initial_params(n0, lambda, n0_count));
+}
+
+int mps_set_initial_params(mps_session *s, double n0, double lambda, int n0_count)
+{
+    MPS_API_BODY(s, s->eng->set_initial_params(n0, lambda, n0_count));
+}
+
+int mps_neighbor_search(mps_session *s) { MPS_API_BODY(s, s->eng->neighbor_search()); }
+
+int mps_step(mps_session *s, int nsteps)
+{
+    if (nsteps < 0) return MPS_ERR_INVALID;
+    MPS_API_BODY(s, s->eng->step(nsteps));
+}
+
+int mps_step_with_list(mps_session *s, const int *neighbors, const int *count, int max_nb)
+{
+    if (!neighbors || !count) return MPS_ERR_INVALID;
+    MPS_API_BODY(s, s->eng->step_with_list(neighbors, count, max_nb));
+}
+
+int mps_get_neighbor_list(mps_session *s, int *neighbors, int *count, int max_nb)
+{
+    MPS_API_BODY(s, s->eng->get_neighbor_list(neighbors, count, max_nb));
+}
+
+int mps_get_cell_index(mps_session *s, int *cell)
+{
+    if (!cell) return MPS_ERR_INVALID;
+    MPS_API_BODY(s, s->eng->get_cell_index(cell));
+}
+
+int mps_get_cell_links(mps_session *s, int *head, int *next, int total_cells)
+{
+    MPS_API_BODY(s, s->eng->get_cell_links(head, next, total_cells));
+}
+
+int mps_get_ppe(mps_session *s, int *eq_idx, int *row_ptr, int *col_idx, double *val, double *b, int *n_eq,
+                long long *nnz)
+{
+    MPS_API_BODY(s, s->eng->get_ppe(eq_idx, row_ptr, col_idx, val, b, n_eq, nnz));
+}
+
+int mps_get_metrics(mps_session *s, mps_metrics_t *m)
+{
+    if (!m) return MPS_ERR_INVALID;
+    MPS_API_BODY(s, *m = s->eng->met);
+}
+
+void *mps_get_stream(mps_session *s) { return (s && s->eng) ? (void *)s->eng->stream() : nullptr; }
+
+const char *mps_last_error(mps_session *s)
+{
+    return (s && s->eng) ? s->eng->last_error.c_str() : "no session";
+}
+
+int mps_run_stage(mps_session *s, int stage, const int *neighbors, const int *count, int max_nb, double arg)
+{
+    MPS_API_BODY(s, s->eng->run_stage(stage, neighbors, count, max_nb, arg));
+}
+
+}  // extern "C"

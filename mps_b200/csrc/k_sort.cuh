@@ -1,0 +1,258 @@
+// k_sort.cuh -- cell binning, counting sort and reorder (the neighbour search).
+//
+// Replaces the reference's cell linked list (neighbor_search.c:146-240).  The
+// reference prepends particles to per-cell chains, so its neighbour lists
+// visit a cell's particles in descending index order.  Here the particles
+// are physically reordered every step by (cell, descending reference index):
+// a histogram of cell counts, an exclusive scan, an atomic scatter into the
+// cell's slot range, and a per-cell rank by index that makes the order within
+// a cell deterministic.  Particles that are not binned (ghosts, outside the
+// grid) go to a trailing bucket in their previous relative order.
+#pragma once
+
+#include "device.cuh"
+
+namespace mps {
+
+// ---- exclusive scan (any length, recursive over block sums) -------------
+
+constexpr int SCAN_THREADS = 512;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+template <class T>
+__global__ void k_scan_tile(const T *__restrict__ in, T *__restrict__ out, T *__restrict__ sums, int n)
+{
+    __shared__ T warp_tot[SCAN_THREADS / 32];
+    int base = blockIdx.x * SCAN_TILE + threadIdx.x * SCAN_ITEMS;
+    T v[SCAN_ITEMS];
+    T run = 0;
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++) {
+        T x = (base + k < n) ? in[base + k] : T(0);
+        v[k] = run;
+        run += x;
+    }
+    // inclusive warp scan of the per-thread totals
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    T inc = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        T y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+    }
+    if (lane == 31) warp_tot[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        T t = (lane < SCAN_THREADS / 32) ? warp_tot[lane] : T(0);
+        T ti = t;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            T y = __shfl_up_sync(0xffffffffu, ti, o);
+            if (lane >= o) ti += y;
+        }
+        if (lane < SCAN_THREADS / 32) warp_tot[lane] = ti - t;   // exclusive
+        if (lane == SCAN_THREADS / 32 - 1 && sums) sums[blockIdx.x] = ti;
+    }
+    __syncthreads();
+    T off = warp_tot[w] + (inc - run);
+#pragma unroll
+    for (int k = 0; k < SCAN_ITEMS; k++)
+        if (base + k < n) out[base + k] = v[k] + off;
+}
+
+template <class T>
+__global__ void k_scan_add(T *__restrict__ out, const T *__restrict__ offs, int n)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += offs[i / SCAN_TILE];
+}
+
+// out[0..n) = exclusive scan of in[0..n); out[n] = total.  `ws` needs
+// scan_workspace(n) elements.
+inline size_t scan_workspace(int n)
+{
+    size_t s = 0;
+    int m = n;
+    while (m > SCAN_TILE) {
+        m = (m + SCAN_TILE - 1) / SCAN_TILE;
+        s += 2 * (size_t)m + 1;
+    }
+    return s + 2;
+}
+
+template <class T>
+__global__ void k_scan_total(const T *in, const T *out, T *tot, int n)
+{
+    if (n == 0) { *tot = 0; return; }
+    *tot = out[n - 1] + in[n - 1];
+}
+
+template <class T>
+void scan_exclusive(const T *in, T *out, int n, T *ws, cudaStream_t st)
+{
+    if (n <= 0) {
+        k_scan_total<T><<<1, 1, 0, st>>>(in, out, out, 0);
+        return;
+    }
+    int nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (nb == 1) {
+        k_scan_tile<T><<<1, SCAN_THREADS, 0, st>>>(in, out, nullptr, n);
+    } else {
+        T *sums = ws;
+        T *sums_scan = ws + nb;   // nb + 1 entries via the recursion
+        k_scan_tile<T><<<nb, SCAN_THREADS, 0, st>>>(in, out, sums, n);
+        scan_exclusive<T>(sums, sums_scan, nb, ws + 2 * nb + 1, st);
+        k_scan_add<T><<<(n + 255) / 256, 256, 0, st>>>(out, sums_scan, n);
+    }
+    k_scan_total<T><<<1, 1, 0, st>>>(in, out, out + n, n);
+}
+
+// ---- binning --------------------------------------------------------------
+
+template <int D>
+__global__ void k_bin(State<D> s, Grid<D> g, int n, int *__restrict__ kcell,
+                      int *__restrict__ count, int *__restrict__ excl)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c = -1;
+    if (s.type[i] != GHOST) {
+        double p[D];
+        load_vec<D>(p, s.pos, i);
+        c = cell_of_pos<D>(g, p);
+    }
+    kcell[i] = c;
+    excl[i] = (c < 0);
+    if (c >= 0) atomicAdd(&count[c], 1);
+}
+
+__global__ void k_scatter(int n, int total, const int *__restrict__ kcell, const int *__restrict__ start,
+                          int *__restrict__ cursor, const int *__restrict__ exoff,
+                          int *__restrict__ tmp, int *__restrict__ perm)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c = kcell[i];
+    if (c >= 0) {
+        int slot = start[c] + atomicAdd(&cursor[c], 1);
+        tmp[slot] = i;
+    } else {
+        perm[start[total] + exoff[i]] = i;
+    }
+}
+
+// Position within the cell = number of cell members with a larger
+// reference index (descending order, as the reference's chains).
+__global__ void k_rank(const int *__restrict__ nbinned, const int *__restrict__ tmp, const int *__restrict__ kcell,
+                       const int *__restrict__ start, const int *__restrict__ id, int *__restrict__ perm)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= *nbinned) return;
+    int i = tmp[t];
+    int c = kcell[i];
+    int me = id[i];
+    int b = start[c], e = start[c + 1];
+    int r = 0;
+    for (int u = b; u < e; u++) r += (id[tmp[u]] > me);
+    perm[b + r] = i;
+}
+
+template <int D>
+__global__ void k_gather(State<D> dst, State<D> src, const int *__restrict__ perm,
+                         const int *__restrict__ kcell, int n, int *__restrict__ where)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    int i = perm[q];
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+        double x = src.pos[d][i];
+        dst.pos[d][q] = x;
+        dst.key[d][q] = x;
+        dst.vel[d][q] = src.vel[d][i];
+        dst.acc[d][q] = src.acc[d][i];
+    }
+    dst.p[q] = src.p[i];
+    dst.n[q] = src.n[i];
+    dst.type[q] = src.type[i];
+    dst.surf[q] = src.surf[i];
+    dst.ncount[q] = src.ncount[i];
+    int id = src.id[i];
+    dst.id[q] = id;
+    dst.cell[q] = kcell[i];
+    where[id] = q;
+}
+
+// Reorder to reference order (engine index == reference index).
+template <int D>
+__global__ void k_unsort(State<D> dst, State<D> src, const int *__restrict__ where, int n)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    int q = where[r];
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+        dst.pos[d][r] = src.pos[d][q];
+        dst.key[d][r] = src.key[d][q];
+        dst.vel[d][r] = src.vel[d][q];
+        dst.acc[d][r] = src.acc[d][q];
+    }
+    dst.p[r] = src.p[q];
+    dst.n[r] = src.n[q];
+    dst.type[r] = src.type[q];
+    dst.surf[r] = src.surf[q];
+    dst.ncount[r] = src.ncount[q];
+    dst.id[r] = r;
+    dst.cell[r] = -1;
+}
+
+// Neighbour list in the reference's layout (rows by reference index,
+// entries as reference indices, reference order).
+template <int D>
+__global__ void k_build_list(CellSource<D> src, const int *__restrict__ id, int n, int max_nb,
+                             int *__restrict__ out_nb, int *__restrict__ out_cnt, unsigned *err)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    int row = id[q];
+    int cnt = 0;
+    size_t base = (size_t)row * (size_t)max_nb;
+    src.for_each(q, [&](int t) {
+        if (cnt < max_nb && out_nb) out_nb[base + cnt] = id[t];
+        cnt++;
+    });
+    if (cnt > max_nb) {
+        atomicOr(err, ERR_NEIGHBOR_OVERFLOW);
+        cnt = max_nb;
+    }
+    out_cnt[row] = cnt;
+}
+
+template <int D>
+__global__ void k_cell_ref_order(const int *__restrict__ cell, const int *__restrict__ id, int n, int *out)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) out[id[q]] = cell[q];
+}
+
+// Compare a caller's list (CSR by reference index, reference indices) with
+// the cell structure's list, entry by entry.
+template <int D>
+__global__ void k_compare_list(CellSource<D> src, const int *__restrict__ id, int n,
+                               const int *__restrict__ lptr, const int *__restrict__ lidx, unsigned *err)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    int row = id[q];
+    int k = lptr[row], e = lptr[row + 1];
+    bool bad = false;
+    src.for_each(q, [&](int t) {
+        if (k >= e || lidx[k] != id[t]) bad = true;
+        k++;
+    });
+    if (k != e) bad = true;
+    if (bad) atomicOr(err, ERR_LIST_MISMATCH);
+}
+
+}  // namespace mps
