@@ -1,0 +1,448 @@
+"""Throughput of the MPS time step on B200: one JSON line on rank 0.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload c1] [--precision fp64]
+
+A step is one full MPS time step (simulation.c:19-118 of the reference) of
+the 3-D dam break named by --workload, device-resident: explicit viscosity
+and collision, the cell-sort neighbour search, number density and surface
+flags, PPE assembly, IC(0) factorisation and the PCG solve to the absolute
+tolerance 1e-9, the pressure gradient and the correction.  `value` is fluid
+particle-steps/s over all ranks (each rank runs an independent replica with
+its own seed: the path does not shard).  The workload's PPE
+matrix alone is ~1.5 GB, far above the 126 MB L2, so consecutive steps do
+not run from cache.
+
+Other keys: `roofline` for the dominant kernel (the CG SpMV, timed with CUDA
+events on the library's stream during the timed steps), `cpu_baseline` (the
+reference compiled from source, OpenMP on all host cores, on a bounded
+sample of the same workload), `e2e` (the same metric through the C ABI with
+host buffers copied in and out every step), `clocks` (nvidia-smi sampled
+during the timed region), `gpu_launches` (kernels this library launched in
+the timed region).
+
+--impl reference times the reference's own CPU implementation (oracle/_ref)
+on the bounded sample, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "3D dam-break particle-steps/s: mixed vs FP64 GPU @ p err≤1e-4; adjoint/fwd cost"
+UNIT = "fluid particle-steps/s"
+
+WORKLOADS = {
+    "c1": "3-D dam break, tank 1.6x0.6x0.6 m, column 0.4x0.6x0.3 m, l0=0.005 m, "
+          "1,170,276 particles (576,000 fluid), dt 5e-4, ICCG tol 1e-9",
+    "c2": "3-D dam break, tank 1.6x0.6x0.6 m, column 0.4x0.6x0.3 m, l0=0.0035 m, dt 3.5e-4, ICCG tol 1e-9",
+}
+# The CPU sample: the same dam break at l0 = 0.01 (225,236 particles,
+# 72,000 fluid); one reference step there is a few seconds on 8 cores,
+# against ~80 s at l0 = 0.005.
+CPU_SAMPLE_L0 = 0.01
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# CPU: the reference compiled from source (oracle/_ref), bounded sample
+# ---------------------------------------------------------------------------
+
+def reference_cpu_steps(steps: int, warmup: int, l0: float = CPU_SAMPLE_L0, seed: int = 0):
+    """Times `steps` reference simulation_step calls (after `warmup` untimed
+    ones) on the sample; returns (fluid particle-steps/s, seconds/step, meta)."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(host_cores()))
+    from mps_b200 import config as CF
+    from mps_b200 import types as T
+    from mps_b200 import workloads as W
+    from oracle.pyoracle import Oracle, Reference
+
+    wl = W.dambreak("c1", l0=l0, seed=seed)
+    cfg = wl.config()
+    kind = "reference"
+    ref = Reference("3d")
+    hp = T.HostParticles(3, wl.pos, wl.vel, wl.types)
+    # n0 / lambda with the oracle's cell-list form of particle.c:69-221 (bit-identical
+    # to the reference's O(N^2) loop, which alone would take minutes here)
+    Oracle(3).initial_params(hp, cfg)
+    ref.set_config(cfg)
+    re = CF.neighbor_radius(cfg)
+    nl = T.HostNeighborList(hp.n, cfg.max_neighbors)
+    cl = ref.cell_list(hp.n, re, cfg)
+    ref.lib.neighbor_search_cell_linked_list(C.byref(nl.nl), C.byref(hp.ps), cl, re)
+    for s in range(warmup):
+        ref.step(hp, nl, cl, s + 1)
+    t0 = time.perf_counter()
+    for s in range(steps):
+        ref.step(hp, nl, cl, warmup + s + 1)
+    dt = time.perf_counter() - t0
+    ref.lib.cell_list_free(cl)
+    meta = {"kind": kind, "cores": int(os.environ["OMP_NUM_THREADS"]),
+            "sample": f"c1 geometry at l0={l0} ({wl.n} particles, {wl.n_fluid} fluid), "
+                      f"{steps} reference simulation_step call(s) after {warmup} warm-up, "
+                      "OpenMP build of mps_fluid3D_parallel compiled from source"}
+    return wl.n_fluid * steps / dt, dt / max(steps, 1), meta
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.3)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# roofline of the dominant kernel
+# ---------------------------------------------------------------------------
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return json.load(fh), "measured"
+    return {"hbm_gbs": 6650.0}, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """Per-launch DRAM bytes of `kernel` from the committed ncu summary
+    (profiles/*.md lines 'traffic_per_launch_bytes <kernel> <bytes> <nnz>'),
+    scaled to this workload's nnz by the bench; None when absent."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for name in sorted(os.listdir(d)):
+        if not name.endswith(".md"):
+            continue
+        for line in open(os.path.join(d, name)):
+            t = line.strip().strip("`").split()
+            if len(t) == 4 and t[0] == "traffic_per_launch_bytes" and t[1] == kernel:
+                return float(t[2]), float(t[3])
+    return None
+
+
+# ---------------------------------------------------------------------------
+# the B200 arm
+# ---------------------------------------------------------------------------
+
+def run_b200(args, rank: int, world: int, local_rank: int):
+    import numpy as np
+    import torch
+
+    from mps_b200 import _lib
+    from mps_b200 import types as T
+    from mps_b200 import workloads as W
+    from mps_b200.session import Session
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    wl = W.dambreak(args.workload, seed=1000 + rank)
+    cfg = wl.config()
+    prec = _lib.PREC_MIXED if args.precision == "mixed" else _lib.PREC_FP64
+    hp = T.HostParticles(3, wl.pos, wl.vel, wl.types)
+    sess = Session(cfg, 3, hp.n, precision=prec)
+    sess.upload(hp)
+    n0, lam, _ = sess.compute_initial_params()
+    sess.neighbor_search()
+    for _ in range(args.warmup):
+        sess.step(1)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(sess.stream)
+    sess.reset_metrics()
+    sess.set_profiling(True)
+    clocks = ClockSampler(local_rank) if rank == 0 else None
+    lib = _lib.load()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    barrier()
+    torch.cuda.synchronize()
+    l0 = lib.mps_launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        sess.step(1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    launches = lib.mps_launch_count() - l0
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop() if clocks else None
+    met = sess.metrics()
+    sess.set_profiling(False)
+
+    # max over ranks of the timed region
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    fluid_total = wl.n_fluid * world
+    value = fluid_total * args.steps / (ms_max / 1e3)
+    iters = met["total_iterations"]
+
+    sess.close()
+    e2e = None if args.no_e2e else run_e2e(wl, cfg, args, torch, dist)
+
+    result = None
+    if rank == 0:
+        peaks, peak_kind = measured_peaks()
+        nnz_mean = met["prof_nnz_sum"] / max(met["prof_iterations"], 1)
+        rows_mean = met["prof_rows_sum"] / max(met["prof_iterations"], 1)
+        # SpMV algorithmic bytes per launch: A values 8 B + column 4 B per
+        # nonzero, row pointer 4 B, p 8 B, Ap 8 B per row.
+        alg_bytes = 12.0 * nnz_mean + 20.0 * rows_mean
+        spmv_ms = met["prof_spmv_ms"] / max(met["prof_spmv_launches"], 1)
+        achieved = alg_bytes / (spmv_ms / 1e3) / 1e9
+        peak = float(peaks.get("hbm_gbs", 6650.0))
+        tr = ncu_traffic("k_cg_spmv")
+        traffic = None
+        if tr is not None:
+            traffic = tr[0] / tr[1] * nnz_mean
+        fwd_ms = met["prof_fwd_ms"] / max(met["prof_fwd_sweeps"], 1)
+        bwd_ms = met["prof_bwd_ms"] / max(met["prof_bwd_sweeps"], 1)
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            v, sec, meta = reference_cpu_steps(args.cpu_steps, 0)
+            cpu = {"value": v, "unit": UNIT, "cores": meta["cores"], "kind": meta["kind"], "sample": meta["sample"],
+                   "seconds_per_step": sec}
+        result = {
+            "metric": METRIC,
+            "value": value,
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64" if prec == _lib.PREC_FP64 else "f32+f64",
+            "data": "synthetic",
+            "config": {
+                "workload": WORKLOADS.get(args.workload, args.workload),
+                "particles_per_gpu": wl.n,
+                "fluid_per_gpu": wl.n_fluid,
+                "precision": args.precision,
+                "parallelism": f"replicas x{world}",
+                "l2": "inputs larger than L2 (PPE matrix ~1.5 GB per replica)",
+                "n0": n0,
+                "lambda": lam,
+            },
+            "total_particle_steps_per_s": wl.n * world * args.steps / (ms_max / 1e3),
+            "ppe_iterations_per_step": iters / args.steps,
+            "ppe_iterations_per_s": iters / (ms_max / 1e3),
+            "stage_ms_last_step": {"ops": met["ms_ops"], "assembly": met["ms_assembly"],
+                                   "factor": met["ms_factor"], "solve": met["ms_solve"]},
+            "kernel_ms_per_launch": {"k_cg_spmv": spmv_ms, "ic0_forward_sweep(8 colours)": fwd_ms,
+                                     "ic0_backward_sweep(8 colours)": bwd_ms,
+                                     "cg_vector_kernels_per_iter": met["prof_vec_ms"] / max(met["prof_iterations"], 1)},
+            "roofline": {"kernel": "k_cg_spmv", "bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": f"{peak_kind} hbm_gbs",
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+    if dist is not None:
+        dist.destroy_process_group()
+    return result
+
+
+def run_e2e(wl, cfg, args, torch, dist):
+    """The same metric through the reference-facing C ABI with host buffers:
+    the drop-in simulation_step(ps, nl, cl, step) of libmps3d.so, whose
+    particles (AoS) and neighbour list live in pinned host memory.  Every
+    call copies the particles and the previous step's list to the device and
+    the new particles, list and cell chains back.  Wall-clock per call, max
+    over ranks."""
+    import numpy as np
+
+    from mps_b200 import config as CF
+    from mps_b200 import types as T
+
+    lib = C.CDLL(os.path.join(ROOT, "mps_b200", "libmps3d.so"))
+    lib.mps_dropin_set_exit_on_error(0)
+    PS = C.POINTER(T.ParticleSystem)
+    NL = C.POINTER(T.NeighborList)
+    CLP = C.POINTER(T.CellList3)
+    lib.particle_system_calc_initial_params.argtypes = [PS]
+    lib.neighbor_search_cell_linked_list.argtypes = [NL, PS, CLP, C.c_double]
+    lib.simulation_step.argtypes = [PS, NL, CLP, C.c_int]
+    lib.cell_list_create.restype = CLP
+    lib.cell_list_create.argtypes = [C.c_int, C.c_double, C.c_void_p, C.c_void_p]
+    lib.mps_dropin_last_status.restype = C.c_int
+    lib.mps_dropin_release.argtypes = [PS]
+    C.c_void_p.in_dll(lib, "g_config").value = C.addressof(cfg)
+
+    n, m = wl.n, cfg.max_neighbors
+    dt_p = T.particle_dtype(3)
+    p_buf = torch.empty(n * dt_p.itemsize, dtype=torch.uint8, pin_memory=True)
+    parts = np.frombuffer(p_buf.numpy(), dtype=dt_p, count=n)
+    parts[:] = 0
+    parts["pos"] = wl.pos
+    parts["vel"] = wl.vel
+    parts["type"] = wl.types
+    ps = T.ParticleSystem()
+    ps.particles = parts.ctypes.data
+    ps.num = ps.capacity = n
+    nb_buf = torch.empty(n * m, dtype=torch.int32, pin_memory=True)
+    cnt_buf = torch.zeros(n, dtype=torch.int32, pin_memory=True)
+    nl = T.NeighborList()
+    nl.neighbors = C.cast(nb_buf.data_ptr(), C.POINTER(C.c_int))
+    nl.count = C.cast(cnt_buf.data_ptr(), C.POINTER(C.c_int))
+    nl.max_neighbors = m
+    re = CF.neighbor_radius(cfg)
+    dmin = (C.c_double * 3)(*cfg.domain_min)
+    dmax = (C.c_double * 3)(*cfg.domain_max)
+    cl = lib.cell_list_create(n, re, C.cast(dmin, C.c_void_p), C.cast(dmax, C.c_void_p))
+    lib.particle_system_calc_initial_params(C.byref(ps))
+    lib.neighbor_search_cell_linked_list(C.byref(nl), C.byref(ps), cl, re)
+    if lib.mps_dropin_last_status() != 0:
+        return None
+    cnt = cnt_buf.numpy()
+    lib.simulation_step(C.byref(ps), C.byref(nl), cl, 1)           # warm-up call
+    steps = args.steps
+    h2d = d2h = 0
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for k in range(steps):
+        mc_in = int(cnt.max())
+        lib.simulation_step(C.byref(ps), C.byref(nl), cl, 2 + k)
+        mc_out = int(cnt.max())
+        # bytes copied by the call: AoS particles and the counts both ways,
+        # the used columns of the list (pitched copy), the cell chains back
+        h2d += n * dt_p.itemsize + 4 * n + 4 * n * mc_in
+        d2h += n * dt_p.itemsize + 4 * n + 4 * n * mc_out + 4 * cl.contents.total_cells + 4 * n
+    wall = time.perf_counter() - t0
+    ok = lib.mps_dropin_last_status() == 0
+    lib.mps_dropin_release(C.byref(ps))
+    t = torch.tensor([wall], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    wall = float(t.item())
+    if not ok:
+        return None
+    world = dist.get_world_size() if dist is not None else 1
+    return {"value": wl.n_fluid * world * steps / wall, "unit": UNIT,
+            "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
+            "ms_per_step": wall / steps * 1e3,
+            "call": "simulation_step(ps, nl, cl, step) of libmps3d.so, pinned host AoS + NeighborList"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local_rank = _env_int("LOCAL_RANK", 0)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        v, sec, meta = reference_cpu_steps(args.steps, args.warmup)
+        line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+                "config": {"workload": WORKLOADS[args.workload] + "; timed on the CPU sample below",
+                           "precision": "fp64", "parallelism": "OpenMP, host cores"},
+                "cpu_baseline": {"value": v, "unit": UNIT, "cores": meta["cores"], "kind": meta["kind"],
+                                 "sample": meta["sample"]},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    res = run_b200(args, rank, world, local_rank)
+    if rank == 0 and res is not None:
+        print(json.dumps(res))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -95,6 +95,20 @@ typedef struct {
     double ms_assembly;
     double ms_factor;
     double ms_solve;
+    /* Per-kernel device time summed over the session while profiling is on
+     * (mps_set_profiling): the SpMV of the CG loop, the forward and backward
+     * colour sweeps of the IC(0) preconditioner, and the CG vector kernels;
+     * only iterations that did work are counted. */
+    double prof_spmv_ms;
+    long long prof_spmv_launches;
+    double prof_fwd_ms;
+    long long prof_fwd_sweeps;
+    double prof_bwd_ms;
+    long long prof_bwd_sweeps;
+    double prof_vec_ms;
+    long long prof_iterations;
+    long long prof_nnz_sum;           /* sum over profiled iterations of nnz */
+    long long prof_rows_sum;          /* sum over profiled iterations of n_eq */
 } mps_metrics_t;
 
 typedef struct mps_session mps_session;
@@ -161,6 +175,14 @@ int  mps_get_ppe(mps_session *s, int *eq_idx, int *row_ptr, int *col_idx, double
 
 int  mps_get_metrics(mps_session *s, mps_metrics_t *m);
 
+/* Kernels launched by this library in this process so far. */
+unsigned long long mps_launch_count(void);
+
+/* Per-kernel timing of the CG loop with CUDA events (adds no host sync). */
+int  mps_set_profiling(mps_session *s, int on);
+/* Zero the accumulated metrics. */
+int  mps_reset_metrics(mps_session *s);
+
 /* The stream all session work is issued on (a cudaStream_t). */
 void *mps_get_stream(mps_session *s);
 
@@ -174,10 +196,11 @@ void *mps_get_stream(mps_session *s);
 #define MPS_STAGE_NEIGHBOR_COUNT 4   /* calc_neighbor_count           (operators.c:226) */
 #define MPS_STAGE_COLLISION      5   /* collision                     (operators.c:371) */
 #define MPS_STAGE_SOLVE_PRESSURE 6   /* solve_pressure                (pressure_solver.c:368) */
-#define MPS_STAGE_SURFACE        7   /* judge_free_surface[_by_count] (operators.c:206,253) */
+#define MPS_STAGE_SURFACE        7   /* judge_free_surface            (operators.c:206); arg = threshold */
 #define MPS_STAGE_CLAMP          8   /* clamp_pressure                (operators.c:188) */
 #define MPS_STAGE_WALL           9   /* apply_wall_boundary           (boundary.c:12) */
 #define MPS_STAGE_OUT_OF_BOUNDS 10   /* remove_out_of_bounds          (boundary.c:33) */
+#define MPS_STAGE_SURFACE_BY_COUNT 11 /* judge_free_surface_by_count (operators.c:253); arg = beta */
 int  mps_run_stage(mps_session *s, int stage, const int *neighbors, const int *count,
                    int max_nb, double arg);
 

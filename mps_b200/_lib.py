@@ -34,6 +34,7 @@ STAGES = {
     "clamp": 8,
     "wall": 9,
     "out_of_bounds": 10,
+    "surface_by_count": 11,
 }
 
 
@@ -89,6 +90,16 @@ class MpsMetrics(C.Structure):
         ("ms_assembly", C.c_double),
         ("ms_factor", C.c_double),
         ("ms_solve", C.c_double),
+        ("prof_spmv_ms", C.c_double),
+        ("prof_spmv_launches", C.c_longlong),
+        ("prof_fwd_ms", C.c_double),
+        ("prof_fwd_sweeps", C.c_longlong),
+        ("prof_bwd_ms", C.c_double),
+        ("prof_bwd_sweeps", C.c_longlong),
+        ("prof_vec_ms", C.c_double),
+        ("prof_iterations", C.c_longlong),
+        ("prof_nnz_sum", C.c_longlong),
+        ("prof_rows_sum", C.c_longlong),
     ]
 
 
@@ -119,6 +130,9 @@ SIGNATURES = {
     "mps_get_ppe": (I, [P, P, P, P, P, P, IP, C.POINTER(C.c_longlong)]),
     "mps_get_metrics": (I, [P, C.POINTER(MpsMetrics)]),
     "mps_get_stream": (P, [P]),
+    "mps_launch_count": (C.c_ulonglong, []),
+    "mps_set_profiling": (I, [P, I]),
+    "mps_reset_metrics": (I, [P]),
     "mps_run_stage": (I, [P, I, P, P, I, C.c_double]),
 }
 

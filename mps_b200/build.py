@@ -24,6 +24,9 @@ FLAGS = ["-lineinfo", "-O3", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC"
 TARGETS = {
     "libmps_b200.so": ["engine.cu"],
 }
+CXX = os.environ.get("MPS_CXX", "g++")
+CC = os.environ.get("MPS_CC", "gcc")
+HOST_FLAGS = ["-O2", "-ffp-contract=off", "-fPIC", "-Wall"]
 
 
 def _stale(out: str, deps) -> bool:
@@ -50,6 +53,33 @@ def build_cuda(force: bool = False, verbose: bool = False) -> list:
     return built
 
 
+def build_host(force: bool = False, verbose: bool = False) -> list:
+    """The drop-in libraries libmps3d.so / libmps2d.so and the mps_sim3d /
+    mps_sim2d command-line drivers, linked against libmps_b200.so."""
+    deps = [os.path.join(CSRC, "dropin.cpp"), os.path.join(CSRC, "mps_sim.c"), os.path.join(HERE, "libmps_b200.so")]
+    deps += glob.glob(os.path.join(ROOT, "include", "*.h"))
+    built = []
+    for dim in (3, 2):
+        lib = os.path.join(HERE, f"libmps{dim}d.so")
+        exe = os.path.join(HERE, f"mps_sim{dim}d")
+        jobs = [
+            (lib, [CXX, *HOST_FLAGS, "-std=c++17", "-shared", f"-DMPS_DIM={dim}", "-o", lib,
+                   os.path.join(CSRC, "dropin.cpp"), f"-L{HERE}", "-lmps_b200", "-Wl,-rpath,$ORIGIN"]),
+            (exe, [CC, *HOST_FLAGS, f"-DMPS_DIM={dim}", "-o", exe, os.path.join(CSRC, "mps_sim.c"),
+                   f"-L{HERE}", f"-lmps{dim}d", "-lmps_b200", "-Wl,-rpath,$ORIGIN"]),
+        ]
+        for out, cmd in jobs:
+            if not force and not _stale(out, deps + ([lib] if out == exe else [])):
+                continue
+            if verbose:
+                print(" ".join(cmd))
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"build failed for {out}:\n{r.stdout}\n{r.stderr}")
+            built.append(out)
+    return built
+
+
 def build_oracle() -> None:
     r = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], capture_output=True, text=True)
     if r.returncode != 0:
@@ -58,6 +88,7 @@ def build_oracle() -> None:
 
 def build_all(force: bool = False, verbose: bool = False) -> None:
     build_cuda(force=force, verbose=verbose)
+    build_host(force=force, verbose=verbose)
     build_oracle()
 
 

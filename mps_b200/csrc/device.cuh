@@ -12,6 +12,21 @@
 
 namespace mps {
 
+// Every kernel of the library is launched through launch(), which counts
+// launches process-wide (mps_launch_count in the C ABI).
+inline unsigned long long &launch_counter()
+{
+    static unsigned long long c = 0;
+    return c;
+}
+
+template <class... KArgs, class... Args>
+inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args... args)
+{
+    kernel<<<grid, block, smem, st>>>(args...);
+    ++launch_counter();
+}
+
 enum : int { FLUID = 0, WALL = 1, GHOST = 2, DUMMY = 3 };
 
 // Device error bits (Engine::err_), turned into MPS_ERR_* codes on the host.

@@ -227,6 +227,8 @@ private:
     CGScalars *sc_host_ = nullptr;
     int *int_host_ = nullptr;
     cudaEvent_t ev_[6];
+    static constexpr int PEV = 5;                 // events per profiled iteration
+    cudaEvent_t pev_[CG_BATCH * PEV];
 
     State<D> &S() { return S_[cur_]; }
     CellSource<D> cells() const
@@ -269,6 +271,7 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
     prm_ = p;
     MPS_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     for (auto &e : ev_) MPS_CUDA(cudaEventCreate(&e));
+    for (auto &e : pev_) MPS_CUDA(cudaEventCreate(&e));
     MPS_CUDA(cudaMallocHost((void **)&sc_host_, sizeof(CGScalars)));
     MPS_CUDA(cudaMallocHost((void **)&int_host_, 16 * sizeof(int)));
     alloc_state();
@@ -312,6 +315,7 @@ Engine<D>::~Engine()
 {
     if (st_) cudaStreamSynchronize(st_);
     for (auto &e : ev_) cudaEventDestroy(e);
+    for (auto &e : pev_) cudaEventDestroy(e);
     if (sc_host_) cudaFreeHost(sc_host_);
     if (int_host_) cudaFreeHost(int_host_);
     if (st_) cudaStreamDestroy(st_);
@@ -508,7 +512,7 @@ void Engine<D>::upload_aos(const void *aos, int num)
     size_t bytes = (size_t)num * AosLayout<D>::size;
     aos_.reserve(bytes + 8);
     MPS_CUDA(cudaMemcpyAsync(aos_.p, aos, bytes, cudaMemcpyHostToDevice, st_));
-    if (num) k_unpack<D><<<nblk(num, TPB), TPB, 0, st_>>>(aos_.p, S(), num);
+    if (num) launch(k_unpack<D>, nblk(num, TPB), TPB, 0, st_, aos_.p, S(), num);
     MPS_CUDA(cudaGetLastError());
     MPS_CUDA(cudaStreamSynchronize(st_));
     structure_ = false;
@@ -521,7 +525,7 @@ void Engine<D>::download_aos(void *aos, int num)
     if (num != n_) throw CudaError("download count differs from the uploaded count", MPS_ERR_INVALID);
     size_t bytes = (size_t)num * AosLayout<D>::size;
     aos_.reserve(bytes + 8);
-    if (num) k_pack<D><<<nblk(num, TPB), TPB, 0, st_>>>(aos_.p, S(), num);
+    if (num) launch(k_pack<D>, nblk(num, TPB), TPB, 0, st_, aos_.p, S(), num);
     MPS_CUDA(cudaGetLastError());
     MPS_CUDA(cudaMemcpyAsync(aos, aos_.p, bytes, cudaMemcpyDeviceToHost, st_));
     MPS_CUDA(cudaStreamSynchronize(st_));
@@ -539,7 +543,7 @@ void Engine<D>::upload_soa(const double *pos, const double *vel, const int *type
                              cudaMemcpyHostToDevice, st_));
     MPS_CUDA(cudaMemcpyAsync(int_in_.p, type, sizeof(int) * num, cudaMemcpyHostToDevice, st_));
     if (num)
-        k_unpack_soa<D><<<nblk(num, TPB), TPB, 0, st_>>>(soa_in_.p, soa_in_.p + (size_t)D * num, int_in_.p, S(),
+        launch(k_unpack_soa<D>, nblk(num, TPB), TPB, 0, st_, soa_in_.p, soa_in_.p + (size_t)D * num, int_in_.p, S(),
                                                          num);
     MPS_CUDA(cudaGetLastError());
     MPS_CUDA(cudaStreamSynchronize(st_));
@@ -552,7 +556,7 @@ void Engine<D>::download_pressure(double *p, int num)
 {
     if (num != n_) throw CudaError("download count differs from the uploaded count", MPS_ERR_INVALID);
     soa_in_.reserve((size_t)num + 2);
-    if (num) k_pressure_ref<D><<<nblk(num, TPB), TPB, 0, st_>>>(S(), num, soa_in_.p);
+    if (num) launch(k_pressure_ref<D>, nblk(num, TPB), TPB, 0, st_, S(), num, soa_in_.p);
     MPS_CUDA(cudaMemcpyAsync(p, soa_in_.p, sizeof(double) * num, cudaMemcpyDeviceToHost, st_));
     MPS_CUDA(cudaStreamSynchronize(st_));
 }
@@ -567,15 +571,15 @@ void Engine<D>::sort()
     State<D> &dst = S_[cur_ ^ 1];
     MPS_CUDA(cudaMemsetAsync(count_.p, 0, sizeof(int) * (total + 1), st_));
     MPS_CUDA(cudaMemsetAsync(cursor_.p, 0, sizeof(int) * (total + 1), st_));
-    if (n) k_bin<D><<<nblk(n, TPB), TPB, 0, st_>>>(src, g_, n, kcell_.p, count_.p, excl_.p);
+    if (n) launch(k_bin<D>, nblk(n, TPB), TPB, 0, st_, src, g_, n, kcell_.p, count_.p, excl_.p);
     scan_exclusive<int>(count_.p, start_.p, total, scanws_.p, st_);
     scan_exclusive<int>(excl_.p, exoff_.p, n, scanws_.p, st_);
     if (n) {
-        k_scatter<<<nblk(n, TPB), TPB, 0, st_>>>(n, total, kcell_.p, start_.p, cursor_.p, exoff_.p, tmp_.p,
+        launch(k_scatter, nblk(n, TPB), TPB, 0, st_, n, total, kcell_.p, start_.p, cursor_.p, exoff_.p, tmp_.p,
                                                  perm_.p);
         // ranks for the binned prefix [0, start[total])
-        k_rank<<<nblk(n, TPB), TPB, 0, st_>>>(start_.p + total, tmp_.p, kcell_.p, start_.p, src.id, perm_.p);
-        k_gather<D><<<nblk(n, TPB), TPB, 0, st_>>>(dst, src, perm_.p, kcell_.p, n, where_.p);
+        launch(k_rank, nblk(n, TPB), TPB, 0, st_, start_.p + total, tmp_.p, kcell_.p, start_.p, src.id, perm_.p);
+        launch(k_gather<D>, nblk(n, TPB), TPB, 0, st_, dst, src, perm_.p, kcell_.p, n, where_.p);
     }
     MPS_CUDA(cudaGetLastError());
     cur_ ^= 1;
@@ -588,7 +592,7 @@ template <int D>
 void Engine<D>::unsort()
 {
     int n = n_;
-    if (n) k_unsort<D><<<nblk(n, TPB), TPB, 0, st_>>>(S_[cur_ ^ 1], S_[cur_], where_.p, n);
+    if (n) launch(k_unsort<D>, nblk(n, TPB), TPB, 0, st_, S_[cur_ ^ 1], S_[cur_], where_.p, n);
     MPS_CUDA(cudaGetLastError());
     cur_ ^= 1;
     structure_ = false;
@@ -602,7 +606,8 @@ void Engine<D>::neighbor_search()
     if (n_) {
         // list lengths only: the reference aborts on overflow during the search
         lcnt_.reserve((size_t)n_ + 1);
-        k_build_list<D><<<nblk(n_, TPB), TPB, 0, st_>>>(cells(), S().id, n_, k_.max_nb, nullptr, lcnt_.p, err_.p);
+        launch(k_build_list<D>, nblk(n_, TPB), TPB, 0, st_, cells(), (const int *)S().id, n_, k_.max_nb, 0,
+               (int *)nullptr, lcnt_.p, err_.p);
     }
     check_err();
 }
@@ -663,14 +668,14 @@ void Engine<D>::compute_initial_params(double *n0, double *lambda, int *n0_count
     MPS_CUDA(cudaMemcpyAsync(dlo.p, lo, sizeof(double) * D, cudaMemcpyHostToDevice, st_));
     MPS_CUDA(cudaMemsetAsync(cnt.p, 0, sizeof(int) * (total + 1), st_));
     MPS_CUDA(cudaMemsetAsync(cur.p, 0, sizeof(int) * (total + 1), st_));
-    k_bbox_cell<D><<<nblk(n, TPB), TPB, 0, st_>>>(S(), n, bg, cs, dlo.p, gcell.p, cnt.p);
+    launch(k_bbox_cell<D>, nblk(n, TPB), TPB, 0, st_, S(), n, bg, cs, dlo.p, gcell.p, cnt.p);
     scan_exclusive<int>(cnt.p, st.p, (int)total, ws.p, st_);
-    k_bbox_scatter<<<nblk(n, TPB), TPB, 0, st_>>>(n, gcell.p, st.p, cur.p, order.p);
+    launch(k_bbox_scatter, nblk(n, TPB), TPB, 0, st_, n, gcell.p, st.p, cur.p, order.p);
     bg.start = st.p;
-    k_initial_params<D><<<nblk(n, 128), 128, 0, st_>>>(S(), n, bg, gcell.p, order.p, rmax, re_n, re_lap,
+    launch(k_initial_params<D>, nblk(n, 128), 128, 0, st_, S(), n, bg, gcell.p, order.p, rmax, re_n, re_lap,
                                                        0.01 * prm_.particle_distance, n0i.p, numi.p, deni.p,
                                                        cnti.p, err_.p);
-    k_initial_argmax<D><<<1, 1024, 0, st_>>>(S(), n, n0i.p, cnti.p, best.p, qbest.p, qbest.p + 1);
+    launch(k_initial_argmax<D>, 1, 1024, 0, st_, S(), n, n0i.p, cnti.p, best.p, qbest.p, qbest.p + 1);
     MPS_CUDA(cudaGetLastError());
     check_err();
     double bv;
@@ -711,29 +716,34 @@ void Engine<D>::set_initial_params(double n0, double lambda, int n0_count)
 
 // ---- the step -------------------------------------------------------------------
 
+// The caller's list (reference layout: row i at nb[i * max_nb], count[i]
+// entries) to CSR on the device: one pitched copy of the used columns, a
+// scan of the counts and a compaction kernel.
 template <int D>
 void Engine<D>::upload_list(const int *nb, const int *cnt, int max_nb)
 {
     int n = n_;
-    std::vector<int> ptr((size_t)n + 1, 0);
+    if (max_nb <= 0) throw CudaError("max_neighbors must be positive", MPS_ERR_INVALID);
+    int mc = 0;
     for (int i = 0; i < n; i++) {
         if (cnt[i] < 0 || cnt[i] > max_nb) throw CudaError("bad neighbour count", MPS_ERR_INVALID);
-        ptr[i + 1] = ptr[i] + cnt[i];
+        mc = std::max(mc, cnt[i]);
     }
-    std::vector<int> idx((size_t)ptr[n] + 1);
-    for (int i = 0; i < n; i++) {
-        const int *row = nb + (size_t)i * max_nb;
-        for (int k = 0; k < cnt[i]; k++) {
-            int j = row[k];
-            if (j < 0 || j >= n) throw CudaError("neighbour index out of range", MPS_ERR_INVALID);
-            idx[(size_t)ptr[i] + k] = j;
-        }
-    }
+    lcnt_.reserve((size_t)n + 1);
     lptr_.reserve((size_t)n + 1);
-    lidx_.reserve(idx.size());
-    MPS_CUDA(cudaMemcpyAsync(lptr_.p, ptr.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice, st_));
-    MPS_CUDA(cudaMemcpyAsync(lidx_.p, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice, st_));
-    MPS_CUDA(cudaStreamSynchronize(st_));
+    MPS_CUDA(cudaMemcpyAsync(lcnt_.p, cnt, sizeof(int) * n, cudaMemcpyHostToDevice, st_));
+    scan_exclusive<int>(lcnt_.p, lptr_.p, n, scanws_.p, st_);
+    if (mc > 0 && n > 0) {
+        lout_.reserve((size_t)n * mc);
+        lidx_.reserve((size_t)n * mc);
+        MPS_CUDA(cudaMemcpy2DAsync(lout_.p, sizeof(int) * mc, nb, sizeof(int) * (size_t)max_nb, sizeof(int) * mc,
+                                   n, cudaMemcpyHostToDevice, st_));
+        launch(k_compact_list, nblk(n, TPB), TPB, 0, st_, (const int *)lout_.p, mc, (const int *)lcnt_.p,
+               (const int *)lptr_.p, n, lidx_.p, err_.p);
+    } else {
+        lidx_.reserve(1);
+    }
+    check_err();
 }
 
 template <int D>
@@ -742,18 +752,18 @@ void Engine<D>::explicit_stage(bool from_list)
     int n = n_;
     if (!n) return;
     int nb = nblk(n, TPB);
-    if (from_list) k_viscosity<D, ListSource><<<nb, TPB, 0, st_>>>(list(), S(), k_, n, 0);
-    else k_viscosity<D, CellSource<D>><<<nb, TPB, 0, st_>>>(cells(), S(), k_, n, 0);
-    k_explicit_update<D><<<nb, TPB, 0, st_>>>(S(), k_, n);
+    if (from_list) launch(k_viscosity<D, ListSource>, nb, TPB, 0, st_, list(), S(), k_, n, 0);
+    else launch(k_viscosity<D, CellSource<D>>, nb, TPB, 0, st_, cells(), S(), k_, n, 0);
+    launch(k_explicit_update<D>, nb, TPB, 0, st_, S(), k_, n);
     if (k_.collision_on) {
         if (D == 3) {
-            if (from_list) k_collision_list<D, ListSource><<<nb, TPB, 0, st_>>>(list(), S(), k_, n, vafter_.p);
-            else k_collision_list<D, CellSource<D>><<<nb, TPB, 0, st_>>>(cells(), S(), k_, n, vafter_.p);
+            if (from_list) launch(k_collision_list<D, ListSource>, nb, TPB, 0, st_, list(), S(), k_, n, vafter_.p);
+            else launch(k_collision_list<D, CellSource<D>>, nb, TPB, 0, st_, cells(), S(), k_, n, vafter_.p);
         } else {
             sort();
-            k_collision_allpairs<D><<<nb, TPB, 0, st_>>>(cells(), S(), k_, n, vafter_.p);
+            launch(k_collision_allpairs<D>, nb, TPB, 0, st_, cells(), S(), k_, n, vafter_.p);
         }
-        k_collision_apply<D><<<nb, TPB, 0, st_>>>(S(), k_, n, vafter_.p);
+        launch(k_collision_apply<D>, nb, TPB, 0, st_, S(), k_, n, vafter_.p);
     }
     MPS_CUDA(cudaGetLastError());
 }
@@ -765,13 +775,13 @@ void Engine<D>::implicit_stage()
     sort();
     if (!n) return;
     int nb = nblk(n, TPB);
-    k_density<D, CellSource<D>><<<nb, TPB, 0, st_>>>(cells(), S(), k_, n, err_.p, 1, 1);
+    launch(k_density<D, CellSource<D>>, nb, TPB, 0, st_, cells(), S(), k_, n, err_.p, 1, 1);
     MPS_CUDA(cudaEventRecord(ev_[1], st_));
     ppe(k_.clamp != 0);
     MPS_CUDA(cudaEventRecord(ev_[4], st_));
-    if (k_.cmps != 2) k_pmin<D, CellSource<D>><<<nb, TPB, 0, st_>>>(cells(), S(), n, pmin_.p);
-    k_gradient<D, CellSource<D>><<<nb, TPB, 0, st_>>>(cells(), S(), k_, n, k_.cmps != 2 ? pmin_.p : nullptr);
-    k_correct<D><<<nb, TPB, 0, st_>>>(S(), k_, n, 1, 1, 1);
+    if (k_.cmps != 2) launch(k_pmin<D, CellSource<D>>, nb, TPB, 0, st_, cells(), S(), n, pmin_.p);
+    launch(k_gradient<D, CellSource<D>>, nb, TPB, 0, st_, cells(), S(), k_, n, k_.cmps != 2 ? pmin_.p : nullptr);
+    launch(k_correct<D>, nb, TPB, 0, st_, S(), k_, n, 1, 1, 1);
     MPS_CUDA(cudaGetLastError());
 }
 
@@ -822,13 +832,13 @@ void Engine<D>::ppe(bool clamp)
     int n = n_, total = g_.total;
     int ncol = 1 << D;
     State<D> &s = S();
-    k_cell_unknowns<D><<<nblk(total, TPB), TPB, 0, st_>>>(s, start_.p, total, ucount_.p);
-    k_color_gather<<<nblk(total, TPB), TPB, 0, st_>>>(ccells_.p, ucount_.p, total, ucol_.p);
+    launch(k_cell_unknowns<D>, nblk(total, TPB), TPB, 0, st_, s, start_.p, total, ucount_.p);
+    launch(k_color_gather, nblk(total, TPB), TPB, 0, st_, ccells_.p, ucount_.p, total, ucol_.p);
     scan_exclusive<int>(ucol_.p, rs_.p, total, scanws_.p, st_);
-    k_assign_rows<D><<<nblk(total, TPB), TPB, 0, st_>>>(s, start_.p, ccells_.p, rs_.p, total, cell_row0_.p,
+    launch(k_assign_rows<D>, nblk(total, TPB), TPB, 0, st_, s, start_.p, ccells_.p, rs_.p, total, cell_row0_.p,
                                                         row_of_.p, part_of_row_.p);
     int nbinned = read_int(start_.p + total);
-    if (n > nbinned) k_offgrid_rows<D><<<nblk(n - nbinned, TPB), TPB, 0, st_>>>(s, nbinned, n, row_of_.p, err_.p);
+    if (n > nbinned) launch(k_offgrid_rows<D>, nblk(n - nbinned, TPB), TPB, 0, st_, s, nbinned, n, row_of_.p, err_.p);
     int n_eq = read_int(rs_.p + total);
     n_eq_ = n_eq;
     met.n_eq = n_eq;
@@ -840,12 +850,12 @@ void Engine<D>::ppe(bool clamp)
         met.nnz = 0;
         MPS_CUDA(cudaEventRecord(ev_[2], st_));
         MPS_CUDA(cudaEventRecord(ev_[3], st_));
-        k_writeback<D><<<nb, TPB, 0, st_>>>(s, row_of_.p, x_.p, n, clamp);
+        launch(k_writeback<D>, nb, TPB, 0, st_, s, row_of_.p, x_.p, n, clamp);
         ppe_valid_ = true;
         return;
     }
     CellSource<D> src = cells();
-    k_row_count<D, CellSource<D>><<<nblk(n_eq, TPB), TPB, 0, st_>>>(src, s, part_of_row_.p, row_of_.p, n_eq,
+    launch(k_row_count<D, CellSource<D>>, nblk(n_eq, TPB), TPB, 0, st_, src, s, part_of_row_.p, row_of_.p, n_eq,
                                                                      rcount_.p);
     scan_exclusive<int>(rcount_.p, row_ptr_.p, n_eq, scanws_.p, st_);
     int nnz = read_int(row_ptr_.p + n_eq);
@@ -855,7 +865,7 @@ void Engine<D>::ppe(bool clamp)
     col_.reserve(nnz);
     A_.reserve(nnz);
     F_.reserve(nnz);
-    k_fill<D><<<nblk(n_eq, 128), 128, 0, st_>>>(src, s, k_, part_of_row_.p, row_of_.p, n_eq, row_ptr_.p, col_.p,
+    launch(k_fill<D>, nblk(n_eq, 128), 128, 0, st_, src, s, k_, part_of_row_.p, row_of_.p, n_eq, row_ptr_.p, col_.p,
                                                 A_.p, diagpos_.p, b_.p, err_.p);
     MPS_CUDA(cudaEventRecord(ev_[2], st_));
     bool icc = prm_.solver_type == 1;
@@ -864,7 +874,7 @@ void Engine<D>::ppe(bool clamp)
         for (int c = 0; c < ncol; c++) {
             int kb = color_off_[c], ke = color_off_[c + 1];
             if (ke > kb)
-                k_ic0_color<<<nblk((long long)(ke - kb) * 32, 256), 256, 0, st_>>>(
+                launch(k_ic0_color, nblk((long long)(ke - kb) * 32, 256), 256, 0, st_, 
                     kb, ke, ccells_.p, cell_row0_.p, ucount_.p, row_ptr_.p, diagpos_.p, col_.p, A_.p, F_.p);
         }
     }
@@ -876,38 +886,90 @@ void Engine<D>::ppe(bool clamp)
     init.maxit = prm_.cg_max_iter;
     MPS_CUDA(cudaMemcpyAsync(sc_.p, &init, sizeof(CGScalars), cudaMemcpyHostToDevice, st_));
     const int RB = RED_BLOCKS;
-    k_cg_init<<<RB, CG_BLOCK, 0, st_>>>(n_eq, x_.p, r_.p, b_.p);
+    launch(k_cg_init, RB, CG_BLOCK, 0, st_, n_eq, x_.p, r_.p, b_.p);
     double *z = icc ? z_.p : r_.p;
     auto precond = [&]() {
         for (int c = 0; c < ncol; c++) {
             int kb = color_off_[c], ke = color_off_[c + 1];
             if (ke > kb)
-                k_fwd_color<<<nblk((long long)(ke - kb) * 32, 256), 256, 0, st_>>>(
+                launch(k_fwd_color, nblk((long long)(ke - kb) * 32, 256), 256, 0, st_, 
                     kb, ke, ccells_.p, cell_row0_.p, ucount_.p, row_ptr_.p, diagpos_.p, col_.p, F_.p, r_.p, y_.p,
                     sc_.p);
         }
         for (int c = ncol - 1; c >= 0; c--) {
             int kb = color_off_[c], ke = color_off_[c + 1];
             if (ke > kb)
-                k_bwd_color<<<nblk((long long)(ke - kb) * 32, 256), 256, 0, st_>>>(
+                launch(k_bwd_color, nblk((long long)(ke - kb) * 32, 256), 256, 0, st_, 
                     kb, ke, ccells_.p, cell_row0_.p, ucount_.p, row_ptr_.p, diagpos_.p, col_.p, F_.p, y_.p, z_.p,
                     sc_.p);
         }
     };
-    if (icc) precond();
-    k_cg_init2<<<RB, CG_BLOCK, 0, st_>>>(n_eq, r_.p, z, p_.p, partials_.p, ticket_.p, sc_.p);
+    auto fwd = [&]() {
+        for (int c = 0; c < ncol; c++) {
+            int kb = color_off_[c], ke = color_off_[c + 1];
+            if (ke > kb)
+                launch(k_fwd_color, nblk((long long)(ke - kb) * 32, 256), 256, 0, st_, 
+                    kb, ke, ccells_.p, cell_row0_.p, ucount_.p, row_ptr_.p, diagpos_.p, col_.p, F_.p, r_.p, y_.p,
+                    sc_.p);
+        }
+    };
+    auto bwd = [&]() {
+        for (int c = ncol - 1; c >= 0; c--) {
+            int kb = color_off_[c], ke = color_off_[c + 1];
+            if (ke > kb)
+                launch(k_bwd_color, nblk((long long)(ke - kb) * 32, 256), 256, 0, st_, 
+                    kb, ke, ccells_.p, cell_row0_.p, ucount_.p, row_ptr_.p, diagpos_.p, col_.p, F_.p, y_.p, z_.p,
+                    sc_.p);
+        }
+    };
+    (void)precond;
+    if (icc) { fwd(); bwd(); }
+    launch(k_cg_init2, RB, CG_BLOCK, 0, st_, n_eq, r_.p, z, p_.p, partials_.p, ticket_.p, sc_.p);
+    int iter_before = 0;
     for (;;) {
+        bool prof = profiling;
         for (int it = 0; it < CG_BATCH; it++) {
-            k_cg_spmv<32><<<RB, CG_BLOCK, 0, st_>>>(n_eq, row_ptr_.p, col_.p, A_.p, p_.p, Ap_.p, partials_.p,
+            cudaEvent_t *e = pev_ + it * PEV;
+            if (prof) MPS_CUDA(cudaEventRecord(e[0], st_));
+            launch(k_cg_spmv<32>, RB, CG_BLOCK, 0, st_, n_eq, row_ptr_.p, col_.p, A_.p, p_.p, Ap_.p, partials_.p,
                                                    ticket_.p, sc_.p);
-            k_cg_axpy<<<RB, CG_BLOCK, 0, st_>>>(n_eq, x_.p, r_.p, p_.p, Ap_.p, partials_.p, ticket_.p, sc_.p);
-            if (icc) precond();
-            k_cg_rz<<<RB, CG_BLOCK, 0, st_>>>(n_eq, r_.p, z, partials_.p, ticket_.p, sc_.p);
-            k_cg_update_p<<<RB, CG_BLOCK, 0, st_>>>(n_eq, p_.p, z, sc_.p);
+            if (prof) MPS_CUDA(cudaEventRecord(e[1], st_));
+            launch(k_cg_axpy, RB, CG_BLOCK, 0, st_, n_eq, x_.p, r_.p, p_.p, Ap_.p, partials_.p, ticket_.p, sc_.p);
+            if (prof) MPS_CUDA(cudaEventRecord(e[2], st_));
+            if (icc) fwd();
+            if (prof) MPS_CUDA(cudaEventRecord(e[3], st_));
+            if (icc) bwd();
+            if (prof) MPS_CUDA(cudaEventRecord(e[4], st_));
+            launch(k_cg_rz, RB, CG_BLOCK, 0, st_, n_eq, r_.p, z, partials_.p, ticket_.p, sc_.p);
+            launch(k_cg_update_p, RB, CG_BLOCK, 0, st_, n_eq, p_.p, z, sc_.p);
         }
         MPS_CUDA(cudaGetLastError());
         MPS_CUDA(cudaMemcpyAsync(sc_host_, sc_.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, st_));
         MPS_CUDA(cudaStreamSynchronize(st_));
+        if (prof) {
+            int worked = sc_host_->iter - iter_before;   // iterations that did work in this batch
+            for (int it = 0; it < worked && it < CG_BATCH; it++) {
+                cudaEvent_t *e = pev_ + it * PEV;
+                float a = 0, b2 = 0, c2 = 0, d2 = 0;
+                cudaEventElapsedTime(&a, e[0], e[1]);
+                cudaEventElapsedTime(&b2, e[1], e[2]);
+                cudaEventElapsedTime(&c2, e[2], e[3]);
+                cudaEventElapsedTime(&d2, e[3], e[4]);
+                met.prof_spmv_ms += a;
+                met.prof_spmv_launches += 1;
+                met.prof_vec_ms += b2;
+                if (icc) {
+                    met.prof_fwd_ms += c2;
+                    met.prof_fwd_sweeps += 1;
+                    met.prof_bwd_ms += d2;
+                    met.prof_bwd_sweeps += 1;
+                }
+                met.prof_iterations += 1;
+                met.prof_nnz_sum += nnz;
+                met.prof_rows_sum += n_eq;
+            }
+        }
+        iter_before = sc_host_->iter;
         if (sc_host_->done) break;
     }
     met.ppe_iterations = sc_host_->iter;
@@ -915,28 +977,43 @@ void Engine<D>::ppe(bool clamp)
     met.ppe_residual = std::sqrt(sc_host_->rr);
     met.converged = std::sqrt(sc_host_->rr) < prm_.cg_tolerance;
     met.total_iterations += sc_host_->iter;
-    k_writeback<D><<<nb, TPB, 0, st_>>>(s, row_of_.p, x_.p, n, clamp);
+    launch(k_writeback<D>, nb, TPB, 0, st_, s, row_of_.p, x_.p, n, clamp);
     MPS_CUDA(cudaGetLastError());
     ppe_valid_ = true;
 }
 
 // ---- introspection --------------------------------------------------------
 
+// The current structure's list into the caller's reference-layout arrays:
+// counts first, then the rows at a pitch of the longest row, copied out with
+// one pitched copy.
 template <int D>
 void Engine<D>::get_neighbor_list(int *nb, int *cnt, int max_nb)
 {
     if (!structure_) throw CudaError("no neighbour structure", MPS_ERR_INVALID);
     int n = n_;
     if (max_nb <= 0) throw CudaError("max_nb must be positive", MPS_ERR_INVALID);
-    size_t slots = (size_t)n * max_nb;
-    if (nb) lout_.reserve(slots + 1);
     lcnt_.reserve((size_t)n + 1);
+    std::vector<int> hc;
+    int *hcnt = cnt;
+    if (!hcnt) {
+        hc.resize((size_t)n + 1);
+        hcnt = hc.data();
+    }
     if (n)
-        k_build_list<D><<<nblk(n, TPB), TPB, 0, st_>>>(cells(), S().id, n, max_nb, nb ? lout_.p : nullptr,
-                                                       lcnt_.p, err_.p);
-    MPS_CUDA(cudaGetLastError());
-    if (nb) MPS_CUDA(cudaMemcpyAsync(nb, lout_.p, sizeof(int) * slots, cudaMemcpyDeviceToHost, st_));
-    if (cnt) MPS_CUDA(cudaMemcpyAsync(cnt, lcnt_.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st_));
+        launch(k_build_list<D>, nblk(n, TPB), TPB, 0, st_, cells(), (const int *)S().id, n, max_nb, 0,
+               (int *)nullptr, lcnt_.p, err_.p);
+    MPS_CUDA(cudaMemcpyAsync(hcnt, lcnt_.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st_));
+    check_err();
+    if (!nb || n == 0) return;
+    int mc = 0;
+    for (int i = 0; i < n; i++) mc = std::max(mc, hcnt[i]);
+    if (mc == 0) return;
+    lout_.reserve((size_t)n * mc);
+    launch(k_build_list<D>, nblk(n, TPB), TPB, 0, st_, cells(), (const int *)S().id, n, max_nb, mc, lout_.p,
+           lcnt_.p, err_.p);
+    MPS_CUDA(cudaMemcpy2DAsync(nb, sizeof(int) * (size_t)max_nb, lout_.p, sizeof(int) * mc, sizeof(int) * mc, n,
+                               cudaMemcpyDeviceToHost, st_));
     check_err();
 }
 
@@ -946,7 +1023,7 @@ void Engine<D>::get_cell_index(int *cell)
     if (!structure_) throw CudaError("no neighbour structure", MPS_ERR_INVALID);
     int n = n_;
     lcnt_.reserve((size_t)n + 1);
-    if (n) k_cell_ref_order<D><<<nblk(n, TPB), TPB, 0, st_>>>(S().cell, S().id, n, lcnt_.p);
+    if (n) launch(k_cell_ref_order<D>, nblk(n, TPB), TPB, 0, st_, S().cell, S().id, n, lcnt_.p);
     MPS_CUDA(cudaMemcpyAsync(cell, lcnt_.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st_));
     MPS_CUDA(cudaStreamSynchronize(st_));
 }
@@ -961,7 +1038,7 @@ void Engine<D>::get_cell_links(int *head, int *next, int total)
     h.reserve(total + 1);
     nx.reserve((size_t)n + 1);
     int m = std::max(total, n);
-    if (m) k_cell_links<<<nblk(m, TPB), TPB, 0, st_>>>(start_.p, S().id, S().cell, total, n, h.p, nx.p);
+    if (m) launch(k_cell_links, nblk(m, TPB), TPB, 0, st_, start_.p, S().id, S().cell, total, n, h.p, nx.p);
     if (head) MPS_CUDA(cudaMemcpyAsync(head, h.p, sizeof(int) * total, cudaMemcpyDeviceToHost, st_));
     if (next) MPS_CUDA(cudaMemcpyAsync(next, nx.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st_));
     MPS_CUDA(cudaStreamSynchronize(st_));
@@ -980,7 +1057,7 @@ void Engine<D>::get_ppe(int *eq_idx, int *row_ptr, int *col, double *val, double
     DevArray<double> cval, cb;
     by_id.reserve(n + 1);
     eq_by_id.reserve(n + 1);
-    if (n) k_ref_eq<<<nblk(n, TPB), TPB, 0, st_>>>(row_of_.p, S().id, n, by_id.p);
+    if (n) launch(k_ref_eq, nblk(n, TPB), TPB, 0, st_, row_of_.p, S().id, n, by_id.p);
     std::vector<int> h_by(n), h_eq(n);
     MPS_CUDA(cudaMemcpyAsync(h_by.data(), by_id.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st_));
     std::vector<int> h_rp(ne + 1);
@@ -1001,7 +1078,7 @@ void Engine<D>::get_ppe(int *eq_idx, int *row_ptr, int *col, double *val, double
     cval.reserve(nnz_ + 1);
     cb.reserve(ne + 1);
     if (ne)
-        k_ppe_to_ref<<<nblk(ne, TPB), TPB, 0, st_>>>(ne, part_of_row_.p, S().id, eq_by_id.p, row_ptr_.p, col_.p,
+        launch(k_ppe_to_ref, nblk(ne, TPB), TPB, 0, st_, ne, part_of_row_.p, S().id, eq_by_id.p, row_ptr_.p, col_.p,
                                                       A_.p, b_.p, part_of_row_.p, rp_ref.p, ccol.p, cval.p, cb.p);
     std::vector<int> hc(nnz_);
     std::vector<double> hv(nnz_);
@@ -1035,63 +1112,65 @@ void Engine<D>::run_stage(int stage, const int *nb, const int *cnt, int max_nb, 
                       stage == MPS_STAGE_NEIGHBOR_COUNT || stage == MPS_STAGE_SOLVE_PRESSURE ||
                       (stage == MPS_STAGE_COLLISION && D == 3);
     bool needs_ref = stage == MPS_STAGE_VISCOSITY || stage == MPS_STAGE_GRADIENT ||
-                     stage == MPS_STAGE_SOLVE_PRESSURE || stage == MPS_STAGE_SURFACE;
+                     stage == MPS_STAGE_SOLVE_PRESSURE || stage == MPS_STAGE_SURFACE ||
+                     stage == MPS_STAGE_SURFACE_BY_COUNT;
     if (needs_ref) require_ref();
     if (needs_list && (!nb || !cnt)) throw CudaError("stage needs a neighbour list", MPS_ERR_INVALID);
     if (structure_ && stage != MPS_STAGE_CLAMP && stage != MPS_STAGE_WALL && stage != MPS_STAGE_OUT_OF_BOUNDS &&
-        stage != MPS_STAGE_SURFACE)
+        stage != MPS_STAGE_SURFACE && stage != MPS_STAGE_SURFACE_BY_COUNT)
         unsort();
     if (needs_list) upload_list(nb, cnt, max_nb);
     int bl = nblk(n, TPB);
     if (n == 0) return;
     switch (stage) {
     case MPS_STAGE_DENSITY:
-        k_density<D, ListSource><<<bl, TPB, 0, st_>>>(list(), S(), k_, n, err_.p, 0, 0);
+        launch(k_density<D, ListSource>, bl, TPB, 0, st_, list(), S(), k_, n, err_.p, 0, 0);
         break;
     case MPS_STAGE_VISCOSITY:
-        k_viscosity<D, ListSource><<<bl, TPB, 0, st_>>>(list(), S(), k_, n, 1);
+        launch(k_viscosity<D, ListSource>, bl, TPB, 0, st_, list(), S(), k_, n, 1);
         break;
     case MPS_STAGE_GRADIENT:
-        if (k_.cmps != 2) k_pmin<D, ListSource><<<bl, TPB, 0, st_>>>(list(), S(), n, pmin_.p);
-        k_gradient<D, ListSource><<<bl, TPB, 0, st_>>>(list(), S(), k_, n, k_.cmps != 2 ? pmin_.p : nullptr);
+        if (k_.cmps != 2) launch(k_pmin<D, ListSource>, bl, TPB, 0, st_, list(), S(), n, pmin_.p);
+        launch(k_gradient<D, ListSource>, bl, TPB, 0, st_, list(), S(), k_, n, k_.cmps != 2 ? pmin_.p : nullptr);
         break;
     case MPS_STAGE_NEIGHBOR_COUNT:
-        k_neighbor_count<D, ListSource><<<bl, TPB, 0, st_>>>(list(), S(), k_, n);
+        launch(k_neighbor_count<D, ListSource>, bl, TPB, 0, st_, list(), S(), k_, n);
         break;
     case MPS_STAGE_COLLISION:
         if (D == 3) {
-            k_collision_list<D, ListSource><<<bl, TPB, 0, st_>>>(list(), S(), k_, n, vafter_.p);
+            launch(k_collision_list<D, ListSource>, bl, TPB, 0, st_, list(), S(), k_, n, vafter_.p);
         } else {
             sort();
-            k_collision_allpairs<D><<<bl, TPB, 0, st_>>>(cells(), S(), k_, n, vafter_.p);
+            launch(k_collision_allpairs<D>, bl, TPB, 0, st_, cells(), S(), k_, n, vafter_.p);
         }
-        k_collision_apply<D><<<bl, TPB, 0, st_>>>(S(), k_, n, vafter_.p);
+        launch(k_collision_apply<D>, bl, TPB, 0, st_, S(), k_, n, vafter_.p);
         break;
     case MPS_STAGE_SOLVE_PRESSURE: {
         // the block-colour solver needs the cell structure; the caller's
         // list must be the one that structure produces
         sort();
-        k_compare_list<D><<<bl, TPB, 0, st_>>>(cells(), S().id, n, lptr_.p, lidx_.p, err_.p);
+        launch(k_compare_list<D>, bl, TPB, 0, st_, cells(), S().id, n, lptr_.p, lidx_.p, err_.p);
         check_err();
         ppe(false);
         break;
     }
-    case MPS_STAGE_SURFACE: {
+    case MPS_STAGE_SURFACE:
+    case MPS_STAGE_SURFACE_BY_COUNT: {
         Consts k = k_;
-        int by_count = prm_.surface_detection_method == 1;
+        int by_count = stage == MPS_STAGE_SURFACE_BY_COUNT;
         if (by_count) k.count_thr = arg * n0_count_;
         else k.surf_thr = arg * n0_;
-        k_surface<D><<<bl, TPB, 0, st_>>>(S(), k, n, by_count);
+        launch(k_surface<D>, bl, TPB, 0, st_, S(), k, n, by_count);
         break;
     }
     case MPS_STAGE_CLAMP:
-        k_clamp<D><<<bl, TPB, 0, st_>>>(S(), n);
+        launch(k_clamp<D>, bl, TPB, 0, st_, S(), n);
         break;
     case MPS_STAGE_WALL:
-        k_correct<D><<<bl, TPB, 0, st_>>>(S(), k_, n, 0, 1, 0);
+        launch(k_correct<D>, bl, TPB, 0, st_, S(), k_, n, 0, 1, 0);
         break;
     case MPS_STAGE_OUT_OF_BOUNDS:
-        k_correct<D><<<bl, TPB, 0, st_>>>(S(), k_, n, 0, 0, 1);
+        launch(k_correct<D>, bl, TPB, 0, st_, S(), k_, n, 0, 0, 1);
         break;
     default:
         throw CudaError("unknown stage", MPS_ERR_INVALID);
@@ -1257,6 +1336,12 @@ int mps_get_metrics(mps_session *s, mps_metrics_t *m)
     if (!m) return MPS_ERR_INVALID;
     MPS_API_BODY(s, *m = s->eng->met);
 }
+
+unsigned long long mps_launch_count(void) { return mps::launch_counter(); }
+
+int mps_set_profiling(mps_session *s, int on) { MPS_API_BODY(s, s->eng->profiling = (on != 0)); }
+
+int mps_reset_metrics(mps_session *s) { MPS_API_BODY(s, s->eng->met = mps_metrics_t{}); }
 
 void *mps_get_stream(mps_session *s) { return (s && s->eng) ? (void *)s->eng->stream() : nullptr; }
 

@@ -69,6 +69,7 @@ public:
                          long long *nnz) = 0;
     virtual void run_stage(int stage, const int *nb, const int *cnt, int max_nb, double arg) = 0;
     virtual cudaStream_t stream() const = 0;
+    bool profiling = false;
     mps_metrics_t met{};
     std::string last_error;
 };

@@ -92,20 +92,20 @@ template <class T>
 void scan_exclusive(const T *in, T *out, int n, T *ws, cudaStream_t st)
 {
     if (n <= 0) {
-        k_scan_total<T><<<1, 1, 0, st>>>(in, out, out, 0);
+        launch(k_scan_total<T>, 1, 1, 0, st, in, out, out, 0);
         return;
     }
     int nb = (n + SCAN_TILE - 1) / SCAN_TILE;
     if (nb == 1) {
-        k_scan_tile<T><<<1, SCAN_THREADS, 0, st>>>(in, out, nullptr, n);
+        launch(k_scan_tile<T>, 1, SCAN_THREADS, 0, st, in, out, nullptr, n);
     } else {
         T *sums = ws;
         T *sums_scan = ws + nb;   // nb + 1 entries via the recursion
-        k_scan_tile<T><<<nb, SCAN_THREADS, 0, st>>>(in, out, sums, n);
+        launch(k_scan_tile<T>, nb, SCAN_THREADS, 0, st, in, out, sums, n);
         scan_exclusive<T>(sums, sums_scan, nb, ws + 2 * nb + 1, st);
-        k_scan_add<T><<<(n + 255) / 256, 256, 0, st>>>(out, sums_scan, n);
+        launch(k_scan_add<T>, (n + 255) / 256, 256, 0, st, out, sums_scan, n);
     }
-    k_scan_total<T><<<1, 1, 0, st>>>(in, out, out + n, n);
+    launch(k_scan_total<T>, 1, 1, 0, st, in, out, out + n, n);
 }
 
 // ---- binning --------------------------------------------------------------
@@ -208,18 +208,19 @@ __global__ void k_unsort(State<D> dst, State<D> src, const int *__restrict__ whe
 }
 
 // Neighbour list in the reference's layout (rows by reference index,
-// entries as reference indices, reference order).
+// entries as reference indices, reference order).  Row r starts at
+// out_nb[r * pitch]; rows longer than max_nb raise the overflow flag.
 template <int D>
-__global__ void k_build_list(CellSource<D> src, const int *__restrict__ id, int n, int max_nb,
+__global__ void k_build_list(CellSource<D> src, const int *__restrict__ id, int n, int max_nb, int pitch,
                              int *__restrict__ out_nb, int *__restrict__ out_cnt, unsigned *err)
 {
     int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) return;
     int row = id[q];
     int cnt = 0;
-    size_t base = (size_t)row * (size_t)max_nb;
+    size_t base = (size_t)row * (size_t)pitch;
     src.for_each(q, [&](int t) {
-        if (cnt < max_nb && out_nb) out_nb[base + cnt] = id[t];
+        if (cnt < pitch && out_nb) out_nb[base + cnt] = id[t];
         cnt++;
     });
     if (cnt > max_nb) {
@@ -227,6 +228,21 @@ __global__ void k_build_list(CellSource<D> src, const int *__restrict__ id, int 
         cnt = max_nb;
     }
     out_cnt[row] = cnt;
+}
+
+// Rows of a pitched host list (already on the device) into CSR.
+__global__ void k_compact_list(const int *__restrict__ rows, int pitch, const int *__restrict__ cnt,
+                               const int *__restrict__ ptr, int n, int *__restrict__ idx, unsigned *err)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c = cnt[i], o = ptr[i];
+    const int *r = rows + (size_t)i * pitch;
+    for (int k = 0; k < c; k++) {
+        int j = r[k];
+        if (j < 0 || j >= n) { atomicOr(err, ERR_LIST_MISMATCH); j = 0; }
+        idx[o + k] = j;
+    }
 }
 
 template <int D>

@@ -144,6 +144,12 @@ class Session:
         self._check(self.lib.mps_get_metrics(self.h, C.byref(m)))
         return {f: getattr(m, f) for f, _ in m._fields_}
 
+    def set_profiling(self, on: bool = True):
+        self._check(self.lib.mps_set_profiling(self.h, int(bool(on))))
+
+    def reset_metrics(self):
+        self._check(self.lib.mps_reset_metrics(self.h))
+
     @property
     def stream(self) -> int:
         return int(self.lib.mps_get_stream(self.h) or 0)
