@@ -207,7 +207,7 @@ def run_b200(args, rank: int, world: int, local_rank: int):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
-    wl = W.dambreak(args.workload, seed=1000 + rank)
+    wl = W.dambreak(args.workload, seed=1000 + rank, l0=args.l0)
     cfg = wl.config()
     prec = _lib.PREC_MIXED if args.precision == "mixed" else _lib.PREC_FP64
     hp = T.HostParticles(3, wl.pos, wl.vel, wl.types)
@@ -418,6 +418,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--l0", type=float, default=None,
+                    help="particle spacing override (smaller cases for profiling)")
     args = ap.parse_args()
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)

@@ -35,6 +35,7 @@ enum : unsigned {
     ERR_UNKNOWN_OFF_GRID  = 2u,   // a PPE unknown outside the cell grid
     ERR_LIST_MISMATCH     = 4u,   // caller list differs from the cell structure
     ERR_COLORING          = 8u,   // matrix couples two same-coloured cells
+    ERR_CELL_OVERFULL     = 16u,  // more than 255 unknowns in one cell
 };
 
 // Constants of one session, evaluated on the host with the reference's

@@ -21,6 +21,7 @@
 #include <array>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <numeric>
@@ -206,16 +207,23 @@ private:
     DevArray<long long> scanws64_;
 
     // ---- block colouring
-    DevArray<int> ccells_;
-    std::vector<int> color_off_;
+    DevArray<int> ccells_, color_off_dev_, aflag_, apos_, acells_, sizes_;
+    std::vector<int> color_off_;   // cells of each colour in ccells_
+    std::vector<int> act_off_;     // cells with unknowns of each colour in acells_
+    std::vector<int> row_off_;     // first row of each colour
+    DevArray<int> inpos_, outpos_, pk_len_lo_, pk_len_up_, pk_off_lo_, pk_off_up_;
+    DevArray<double> pk_val_lo_, pk_val_up_, dinv_;
+    DevArray<unsigned char> pk_k_lo_, pk_k_up_;
+    DevArray<int2> adesc_;
 
     // ---- PPE
     DevArray<int> ucount_, ucol_, rs_, cell_row0_, row_of_, part_of_row_, rcount_, row_ptr_, diagpos_, col_;
-    DevArray<double> A_, F_, b_, x_, r_, z_, p_, Ap_, y_, partials_;
+    DevArray<double> A_, F_, b_, x_, r_, z_, p_, Ap_, y_, part_, partials_;
     DevArray<CGScalars> sc_;
     DevArray<unsigned> ticket_, err_;
     int n_eq_ = 0;
     long long nnz_ = 0;
+    int spmv_lpr_ = 8;   // lanes per row of the CG SpMV (MPS_SPMV_LPR: 8, 16 or 32)
     bool ppe_valid_ = false;
 
     // ---- misc
@@ -269,11 +277,15 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
     if (p.surface_tension_enabled) throw CudaError("surface tension is not on this path", MPS_ERR_UNSUPPORTED);
     cap_ = capacity;
     prm_ = p;
+    if (const char *e = std::getenv("MPS_SPMV_LPR")) {
+        int v = std::atoi(e);
+        if (v == 8 || v == 16 || v == 32) spmv_lpr_ = v;
+    }
     MPS_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     for (auto &e : ev_) MPS_CUDA(cudaEventCreate(&e));
     for (auto &e : pev_) MPS_CUDA(cudaEventCreate(&e));
     MPS_CUDA(cudaMallocHost((void **)&sc_host_, sizeof(CGScalars)));
-    MPS_CUDA(cudaMallocHost((void **)&int_host_, 16 * sizeof(int)));
+    MPS_CUDA(cudaMallocHost((void **)&int_host_, 64 * sizeof(int)));
     alloc_state();
     build_grid();
     compute_consts();
@@ -358,7 +370,11 @@ void Engine<D>::alloc_state()
     rcount_.reserve(cap_ + 1);
     row_ptr_.reserve(cap_ + 1);
     diagpos_.reserve(cap_);
-    for (auto *v : {&b_, &x_, &r_, &z_, &p_, &Ap_, &y_}) v->reserve(cap_);
+    inpos_.reserve(cap_);
+    outpos_.reserve(cap_);
+    for (auto *v : {&pk_len_lo_, &pk_len_up_, &pk_off_lo_, &pk_off_up_}) v->reserve((size_t)cap_ + 1);
+    dinv_.reserve(cap_);
+    for (auto *v : {&b_, &x_, &r_, &z_, &p_, &Ap_, &y_, &part_}) v->reserve(cap_);
 }
 
 // cell_list_create (neighbor_search.c:92-122) with cell size = list radius.
@@ -408,6 +424,12 @@ void Engine<D>::build_grid()
     for (long long l = 0; l < total; l++) cc[(size_t)fill[color_of(l)]++] = (int)l;
     ccells_.reserve(total);
     MPS_CUDA(cudaMemcpy(ccells_.p, cc.data(), sizeof(int) * (size_t)total, cudaMemcpyHostToDevice));
+    color_off_dev_.reserve(ncol + 1);
+    MPS_CUDA(cudaMemcpy(color_off_dev_.p, color_off_.data(), sizeof(int) * (ncol + 1), cudaMemcpyHostToDevice));
+    aflag_.reserve(total + 1);
+    apos_.reserve(total + 1);
+    acells_.reserve(total + 1);
+    sizes_.reserve(16);
 }
 
 // Constants evaluated with the reference's expressions.
@@ -498,6 +520,7 @@ void Engine<D>::check_err()
         if (e & ERR_UNKNOWN_OFF_GRID) throw CudaError("a PPE unknown lies outside the cell grid", MPS_ERR_UNSUPPORTED);
         if (e & ERR_LIST_MISMATCH) throw CudaError("neighbour list does not match the cell structure", MPS_ERR_UNSUPPORTED);
         if (e & ERR_COLORING) throw CudaError("PPE row count mismatch", MPS_ERR_INVALID);
+        if (e & ERR_CELL_OVERFULL) throw CudaError("more than 255 PPE unknowns in one cell", MPS_ERR_UNSUPPORTED);
         throw CudaError("device error", MPS_ERR_INVALID);
     }
 }
@@ -835,11 +858,22 @@ void Engine<D>::ppe(bool clamp)
     launch(k_cell_unknowns<D>, nblk(total, TPB), TPB, 0, st_, s, start_.p, total, ucount_.p);
     launch(k_color_gather, nblk(total, TPB), TPB, 0, st_, ccells_.p, ucount_.p, total, ucol_.p);
     scan_exclusive<int>(ucol_.p, rs_.p, total, scanws_.p, st_);
-    launch(k_assign_rows<D>, nblk(total, TPB), TPB, 0, st_, s, start_.p, ccells_.p, rs_.p, total, cell_row0_.p,
-                                                        row_of_.p, part_of_row_.p);
-    int nbinned = read_int(start_.p + total);
-    if (n > nbinned) launch(k_offgrid_rows<D>, nblk(n - nbinned, TPB), TPB, 0, st_, s, nbinned, n, row_of_.p, err_.p);
-    int n_eq = read_int(rs_.p + total);
+    launch(k_assign_rows<D>, nblk(total, TPB), TPB, 0, st_, s, (const int *)start_.p, (const int *)ccells_.p,
+           (const int *)rs_.p, total, cell_row0_.p, row_of_.p, part_of_row_.p);
+    launch(k_active_flag, nblk(total, TPB), TPB, 0, st_, (const int *)ucol_.p, total, aflag_.p);
+    scan_exclusive<int>(aflag_.p, apos_.p, total, scanws_.p, st_);
+    launch(k_active_scatter, nblk(total, TPB), TPB, 0, st_, (const int *)ccells_.p, (const int *)ucol_.p,
+           (const int *)apos_.p, total, acells_.p);
+    launch(k_ppe_sizes, 1, 1, 0, st_, (const int *)rs_.p, (const int *)apos_.p, (const int *)start_.p, total,
+           (const int *)color_off_dev_.p, ncol, sizes_.p);
+    MPS_CUDA(cudaMemcpyAsync(int_host_, sizes_.p, sizeof(int) * (2 * ncol + 4), cudaMemcpyDeviceToHost, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+    int n_eq = int_host_[0];
+    int nbinned = int_host_[1];
+    act_off_.assign(int_host_ + 2, int_host_ + 3 + ncol);
+    row_off_.assign(int_host_ + 3 + ncol, int_host_ + 4 + 2 * ncol);
+    if (n > nbinned)
+        launch(k_offgrid_rows<D>, nblk(n - nbinned, TPB), TPB, 0, st_, s, nbinned, n, row_of_.p, err_.p);
     n_eq_ = n_eq;
     met.n_eq = n_eq;
     int nb = nblk(n, TPB);
@@ -870,13 +904,42 @@ void Engine<D>::ppe(bool clamp)
     MPS_CUDA(cudaEventRecord(ev_[2], st_));
     bool icc = prm_.solver_type == 1;
     if (icc) {
+        launch(k_row_splits, nblk(n_eq, TPB), TPB, 0, st_, n_eq, (const int *)row_ptr_.p, (const int *)diagpos_.p,
+               (const int *)col_.p, (const int *)part_of_row_.p, (const int *)s.cell, (const int *)cell_row0_.p,
+               (const int *)ucount_.p, inpos_.p, outpos_.p);
         MPS_CUDA(cudaMemcpyAsync(F_.p, A_.p, sizeof(double) * nnz, cudaMemcpyDeviceToDevice, st_));
         for (int c = 0; c < ncol; c++) {
-            int kb = color_off_[c], ke = color_off_[c + 1];
+            int rb = row_off_[c], re = row_off_[c + 1];
+            if (re > rb)
+                launch(k_ic0_cross, nblk(re - rb, 128), 128, 0, st_, rb, re, (const int *)row_ptr_.p,
+                       (const int *)diagpos_.p, (const int *)inpos_.p, (const int *)col_.p, (const double *)A_.p,
+                       F_.p);
+            int kb = act_off_[c], ke = act_off_[c + 1];
             if (ke > kb)
-                launch(k_ic0_color, nblk((long long)(ke - kb) * 32, 256), 256, 0, st_, 
-                    kb, ke, ccells_.p, cell_row0_.p, ucount_.p, row_ptr_.p, diagpos_.p, col_.p, A_.p, F_.p);
+                launch(k_ic0_incell, nblk(ke - kb, SWEEP_WARPS_IC), 32 * SWEEP_WARPS_IC, 0, st_, kb, ke,
+                       (const int *)acells_.p, (const int *)cell_row0_.p, (const int *)ucount_.p,
+                       (const int *)row_ptr_.p, (const int *)diagpos_.p, (const int *)inpos_.p,
+                       (const int *)col_.p, (const double *)A_.p, F_.p);
         }
+        // packed in-cell factor and cell descriptors for the sweeps
+        launch(k_pack_lengths, nblk(n_eq, TPB), TPB, 0, st_, n_eq, (const int *)row_ptr_.p,
+               (const int *)diagpos_.p, (const int *)inpos_.p, (const int *)outpos_.p, pk_len_lo_.p, pk_len_up_.p);
+        scan_exclusive<int>(pk_len_lo_.p, pk_off_lo_.p, n_eq, scanws_.p, st_);
+        scan_exclusive<int>(pk_len_up_.p, pk_off_up_.p, n_eq, scanws_.p, st_);
+        size_t in_cap = (size_t)nnz;   // in-cell entries are a subset of the nonzeros
+        pk_val_lo_.reserve(in_cap);
+        pk_val_up_.reserve(in_cap);
+        pk_k_lo_.reserve(in_cap);
+        pk_k_up_.reserve(in_cap);
+        launch(k_pack_fill, nblk(n_eq, TPB), TPB, 0, st_, n_eq, (const int *)diagpos_.p, (const int *)inpos_.p,
+               (const int *)outpos_.p, (const int *)col_.p, (const double *)F_.p, (const int *)part_of_row_.p,
+               (const int *)s.cell, (const int *)cell_row0_.p, (const int *)pk_off_lo_.p,
+               (const int *)pk_off_up_.p, pk_val_lo_.p, pk_k_lo_.p, pk_val_up_.p, pk_k_up_.p, dinv_.p, err_.p);
+        int nact = act_off_[ncol];
+        adesc_.reserve((size_t)nact + 1);
+        if (nact)
+            launch(k_cell_desc, nblk(nact, TPB), TPB, 0, st_, nact, (const int *)acells_.p,
+                   (const int *)cell_row0_.p, (const int *)ucount_.p, adesc_.p);
     }
     MPS_CUDA(cudaEventRecord(ev_[3], st_));
 
@@ -888,41 +951,48 @@ void Engine<D>::ppe(bool clamp)
     const int RB = RED_BLOCKS;
     launch(k_cg_init, RB, CG_BLOCK, 0, st_, n_eq, x_.p, r_.p, b_.p);
     double *z = icc ? z_.p : r_.p;
-    auto precond = [&]() {
-        for (int c = 0; c < ncol; c++) {
-            int kb = color_off_[c], ke = color_off_[c + 1];
-            if (ke > kb)
-                launch(k_fwd_color, nblk((long long)(ke - kb) * 32, 256), 256, 0, st_, 
-                    kb, ke, ccells_.p, cell_row0_.p, ucount_.p, row_ptr_.p, diagpos_.p, col_.p, F_.p, r_.p, y_.p,
-                    sc_.p);
-        }
-        for (int c = ncol - 1; c >= 0; c--) {
-            int kb = color_off_[c], ke = color_off_[c + 1];
-            if (ke > kb)
-                launch(k_bwd_color, nblk((long long)(ke - kb) * 32, 256), 256, 0, st_, 
-                    kb, ke, ccells_.p, cell_row0_.p, ucount_.p, row_ptr_.p, diagpos_.p, col_.p, F_.p, y_.p, z_.p,
-                    sc_.p);
-        }
-    };
+    // IC(0) sweeps, per colour: cross-cell products of all its rows, then the
+    // in-cell solve a warp per cell.
     auto fwd = [&]() {
         for (int c = 0; c < ncol; c++) {
-            int kb = color_off_[c], ke = color_off_[c + 1];
-            if (ke > kb)
-                launch(k_fwd_color, nblk((long long)(ke - kb) * 32, 256), 256, 0, st_, 
-                    kb, ke, ccells_.p, cell_row0_.p, ucount_.p, row_ptr_.p, diagpos_.p, col_.p, F_.p, r_.p, y_.p,
-                    sc_.p);
+            int rb = row_off_[c], re = row_off_[c + 1];
+            if (re <= rb) continue;
+            launch(k_sweep_cross<true, 8>, nblk((long long)(re - rb) * 8, 256), 256, 0, st_, rb, re,
+                   (const int *)row_ptr_.p, (const int *)inpos_.p, (const int *)outpos_.p, (const int *)col_.p,
+                   (const double *)F_.p, (const double *)r_.p, (const double *)y_.p, part_.p,
+                   (const CGScalars *)sc_.p);
+            int kb = act_off_[c], ke = act_off_[c + 1];
+            launch(k_sweep_cell<true>, nblk(ke - kb, CELL_WARPS), 32 * CELL_WARPS, 0, st_, kb, ke,
+                   (const int2 *)adesc_.p, (const int *)pk_off_lo_.p, (const int *)pk_len_lo_.p,
+                   (const double *)pk_val_lo_.p, (const unsigned char *)pk_k_lo_.p, (const double *)dinv_.p,
+                   (const double *)part_.p, y_.p, (const CGScalars *)sc_.p);
         }
     };
     auto bwd = [&]() {
         for (int c = ncol - 1; c >= 0; c--) {
-            int kb = color_off_[c], ke = color_off_[c + 1];
-            if (ke > kb)
-                launch(k_bwd_color, nblk((long long)(ke - kb) * 32, 256), 256, 0, st_, 
-                    kb, ke, ccells_.p, cell_row0_.p, ucount_.p, row_ptr_.p, diagpos_.p, col_.p, F_.p, y_.p, z_.p,
-                    sc_.p);
+            int rb = row_off_[c], re = row_off_[c + 1];
+            if (re <= rb) continue;
+            launch(k_sweep_cross<false, 8>, nblk((long long)(re - rb) * 8, 256), 256, 0, st_, rb, re,
+                   (const int *)row_ptr_.p, (const int *)inpos_.p, (const int *)outpos_.p, (const int *)col_.p,
+                   (const double *)F_.p, (const double *)y_.p, (const double *)z_.p, part_.p,
+                   (const CGScalars *)sc_.p);
+            int kb = act_off_[c], ke = act_off_[c + 1];
+            launch(k_sweep_cell<false>, nblk(ke - kb, CELL_WARPS), 32 * CELL_WARPS, 0, st_, kb, ke,
+                   (const int2 *)adesc_.p, (const int *)pk_off_up_.p, (const int *)pk_len_up_.p,
+                   (const double *)pk_val_up_.p, (const unsigned char *)pk_k_up_.p, (const double *)dinv_.p,
+                   (const double *)part_.p, z_.p, (const CGScalars *)sc_.p);
         }
     };
-    (void)precond;
+    auto spmv = [&](int ne) {
+        const int *rp = row_ptr_.p, *ci = col_.p;
+        const double *av = A_.p, *pv = p_.p;
+        if (spmv_lpr_ == 8)
+            launch(k_cg_spmv<8>, RB, CG_BLOCK, 0, st_, ne, rp, ci, av, pv, Ap_.p, partials_.p, ticket_.p, sc_.p);
+        else if (spmv_lpr_ == 16)
+            launch(k_cg_spmv<16>, RB, CG_BLOCK, 0, st_, ne, rp, ci, av, pv, Ap_.p, partials_.p, ticket_.p, sc_.p);
+        else
+            launch(k_cg_spmv<32>, RB, CG_BLOCK, 0, st_, ne, rp, ci, av, pv, Ap_.p, partials_.p, ticket_.p, sc_.p);
+    };
     if (icc) { fwd(); bwd(); }
     launch(k_cg_init2, RB, CG_BLOCK, 0, st_, n_eq, r_.p, z, p_.p, partials_.p, ticket_.p, sc_.p);
     int iter_before = 0;
@@ -931,8 +1001,7 @@ void Engine<D>::ppe(bool clamp)
         for (int it = 0; it < CG_BATCH; it++) {
             cudaEvent_t *e = pev_ + it * PEV;
             if (prof) MPS_CUDA(cudaEventRecord(e[0], st_));
-            launch(k_cg_spmv<32>, RB, CG_BLOCK, 0, st_, n_eq, row_ptr_.p, col_.p, A_.p, p_.p, Ap_.p, partials_.p,
-                                                   ticket_.p, sc_.p);
+            spmv(n_eq);
             if (prof) MPS_CUDA(cudaEventRecord(e[1], st_));
             launch(k_cg_axpy, RB, CG_BLOCK, 0, st_, n_eq, x_.p, r_.p, p_.p, Ap_.p, partials_.p, ticket_.p, sc_.p);
             if (prof) MPS_CUDA(cudaEventRecord(e[2], st_));

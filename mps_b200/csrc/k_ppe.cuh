@@ -66,6 +66,30 @@ __global__ void k_color_gather(const int *__restrict__ ccells, const int *__rest
     if (k < total) ucol[k] = ucount[ccells[k]];
 }
 
+// Cells holding unknowns, in colour order: flag, scan, scatter.
+__global__ void k_active_flag(const int *__restrict__ ucol, int total, int *__restrict__ flag)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < total) flag[k] = ucol[k] > 0;
+}
+
+__global__ void k_active_scatter(const int *__restrict__ ccells, const int *__restrict__ ucol,
+                                 const int *__restrict__ apos, int total, int *__restrict__ acells)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < total && ucol[k] > 0) acells[apos[k]] = ccells[k];
+}
+
+// Row counts and colour offsets read back in one copy.
+__global__ void k_ppe_sizes(const int *__restrict__ rs, const int *__restrict__ apos, const int *__restrict__ start,
+                            int total, const int *__restrict__ color_off, int ncol, int *__restrict__ out)
+{
+    out[0] = rs[total];        // n_eq
+    out[1] = start[total];     // binned particles
+    for (int c = 0; c <= ncol; c++) out[2 + c] = apos[color_off[c]];             // active cells per colour
+    for (int c = 0; c <= ncol; c++) out[3 + ncol + c] = rs[color_off[c]];        // rows per colour
+}
+
 template <int D>
 __global__ void k_assign_rows(State<D> s, const int *__restrict__ start, const int *__restrict__ ccells,
                               const int *__restrict__ rs, int total, int *__restrict__ cell_row0,
@@ -242,6 +266,9 @@ __global__ void k_fill(CellSource<D> src, State<D> s, Consts k, const int *__res
 // diagonal slot holds 1/L_ii, and above the diagonal F[p] = L_ki (the
 // transposed copy the backward sweep reads row-wise).
 
+constexpr int IC_MAXM = 128;
+constexpr int SWEEP_WARPS_IC = 4;
+
 __device__ __forceinline__ int find_col(const int *__restrict__ col, int lo, int hi, int key)
 {
     while (lo < hi) {
@@ -260,94 +287,449 @@ __device__ __forceinline__ double warp_allsum(double v)
     return v;
 }
 
-// One warp per cell of the colour; the cell's rows in order.
-__global__ void k_ic0_color(int kbeg, int kend, const int *__restrict__ ccells, const int *__restrict__ cell_row0,
-                            const int *__restrict__ ucount, const int *__restrict__ row_ptr,
-                            const int *__restrict__ diagpos, const int *__restrict__ col,
+// Entry L_rk = (A_rk - sum_{j<k} L_rj L_kj) / L_kk of row r at position p
+// (column k), with the sum in ascending j as pressure_solver.c:203-219; the
+// transposed copy goes to row k's upper run.
+__device__ __forceinline__ void ic0_entry(int r, int p, const int *__restrict__ row_ptr,
+                                          const int *__restrict__ diagpos, const int *__restrict__ col,
+                                          const double *__restrict__ A, double *F)
+{
+    int kc = col[p];
+    int a = row_ptr[r], b = row_ptr[kc], kd = diagpos[kc];
+    double s = A[p];
+    while (a < p && b < kd) {
+        int ja = col[a], jb = col[b];
+        if (ja < jb) a++;
+        else if (ja > jb) b++;
+        else { s -= F[a] * F[b]; a++; b++; }
+    }
+    double lik = s * F[kd];
+    F[p] = lik;
+    int up = find_col(col, kd + 1, row_ptr[kc + 1], r);
+    if (up >= 0) F[up] = lik;
+}
+
+__device__ __forceinline__ void ic0_diag(int r, const int *__restrict__ row_ptr, const int *__restrict__ diagpos,
+                                         const double *__restrict__ A, double *F)
+{
+    int pd = diagpos[r];
+    double a = A[pd];
+    double d = a;
+    for (int q = row_ptr[r]; q < pd; q++) d -= F[q] * F[q];
+    if (d <= 0.0) d = (a > 0.0) ? a : 1.0e-30;   // pressure_solver.c:200
+    F[pd] = 1.0 / sqrt(d);
+}
+
+// Phase A of a colour: the cross-cell entries of its rows [rbeg, rend),
+// which depend only on finished colours and on earlier entries of the same
+// row.  Thread per row.
+__global__ void k_ic0_cross(int rbeg, int rend, const int *__restrict__ row_ptr, const int *__restrict__ diagpos,
+                            const int *__restrict__ inpos, const int *__restrict__ col,
                             const double *__restrict__ A, double *F)
 {
-    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int r = rbeg + blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rend) return;
+    int pin = inpos[r];
+    for (int p = row_ptr[r]; p < pin; p++) ic0_entry(r, p, row_ptr, diagpos, col, A, F);
+}
+
+// Phase B of a colour: in-cell entries and diagonals.  Warp per cell; lane l
+// owns rows l, l+32, ...  At step k the owner of row k (complete by then)
+// forms its diagonal, then every row with an entry in column k computes it.
+__global__ void __launch_bounds__(32 * SWEEP_WARPS_IC)
+k_ic0_incell(int kbeg, int kend, const int *__restrict__ acells, const int *__restrict__ cell_row0,
+             const int *__restrict__ ucount, const int *__restrict__ row_ptr, const int *__restrict__ diagpos,
+             const int *__restrict__ inpos, const int *__restrict__ col, const double *__restrict__ A, double *F)
+{
     int lane = threadIdx.x & 31;
-    int kk = kbeg + warp;
+    int kk = kbeg + blockIdx.x * SWEEP_WARPS_IC + (threadIdx.x >> 5);
     if (kk >= kend) return;
-    int c = ccells[kk];
+    int c = acells[kk];
     int r0 = cell_row0[c], m = ucount[c];
-    for (int r = r0; r < r0 + m; r++) {
-        int p0 = row_ptr[r], pd = diagpos[r];
-        for (int p = p0; p < pd; p++) {
-            int kc = col[p];
-            int k0 = row_ptr[kc], kd = diagpos[kc];
-            double part = 0.0;
-            for (int q = p0 + lane; q < p; q += 32) {
-                int pos = find_col(col, k0, kd, col[q]);
-                if (pos >= 0) part += F[q] * F[pos];
+    if (m > IC_MAXM) {
+        if (lane == 0) {
+            for (int r = r0; r < r0 + m; r++) {
+                for (int p = inpos[r]; p < diagpos[r]; p++) ic0_entry(r, p, row_ptr, diagpos, col, A, F);
+                ic0_diag(r, row_ptr, diagpos, A, F);
             }
-            double s = A[p] - warp_allsum(part);
-            double lik = s * F[kd];
-            if (lane == 0) {
-                F[p] = lik;
-                int up = find_col(col, kd + 1, row_ptr[kc + 1], r);
-                if (up >= 0) F[up] = lik;
-            }
-            __syncwarp();
         }
-        double part = 0.0;
-        for (int q = p0 + lane; q < pd; q += 32) part += F[q] * F[q];
-        double a = A[pd];
-        double d = a - warp_allsum(part);
-        if (d <= 0.0) d = (a > 0.0) ? a : 1.0e-30;
-        if (lane == 0) F[pd] = 1.0 / sqrt(d);
+        __syncwarp();
+        return;
+    }
+    constexpr int R = IC_MAXM / 32;
+    int cur[R], stop[R], ccol[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        int t = lane + 32 * j;
+        cur[j] = stop[j] = 0;
+        ccol[j] = -1;
+        if (t < m) {
+            cur[j] = inpos[r0 + t];
+            stop[j] = diagpos[r0 + t];
+            if (cur[j] < stop[j]) ccol[j] = col[cur[j]];
+        }
+    }
+    for (int k = 0; k < m; k++) {
+        if (lane == (k & 31)) ic0_diag(r0 + k, row_ptr, diagpos, A, F);
+        __syncwarp();
+        int ck = r0 + k;
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            if (ccol[j] == ck) {
+                ic0_entry(r0 + lane + 32 * j, cur[j], row_ptr, diagpos, col, A, F);
+                cur[j]++;
+                ccol[j] = (cur[j] < stop[j]) ? col[cur[j]] : -1;
+            }
+        }
         __syncwarp();
     }
 }
 
 // ---- preconditioner sweeps ------------------------------------------------
+//
+// Rows of a cell are contiguous, [r0, r0 + m), and the sorted columns of a
+// row split into four runs: lower cross-cell (earlier colours, col < r0),
+// lower in-cell (r0 <= col < row), the diagonal, upper in-cell, upper
+// cross-cell (col >= r0 + m).  `inpos[r]` is the first in-cell position and
+// `outpos[r]` the first upper cross-cell position of row r.
+//
+// A sweep over one colour runs a warp per cell in two phases:
+//   1. the cross-cell products of every row of the cell, which depend only on
+//      finished colours: 8 lanes per row, 4 rows at a time, into shared memory;
+//   2. the in-cell triangular solve: lane l owns rows l, l+32, ...; at step k
+//      the owner of row k finishes it and broadcasts the value with a
+//      shuffle, and every lane whose row has an entry in column k applies it
+//      (each lane walks its row's in-cell run with a cursor).
+// Cells with more than SWEEP_MAXM unknowns (4x the rest density; only in a
+// blow-up) take a row-by-row path with the same result.
+
+constexpr int SWEEP_MAXM = 128;
+constexpr int SWEEP_WARPS = 4;   // warps per block
+
+// Row positions of the in-cell runs; one thread per row.
+__global__ void k_row_splits(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ diagpos,
+                             const int *__restrict__ col, const int *__restrict__ part_of_row,
+                             const int *__restrict__ cell, const int *__restrict__ cell_row0,
+                             const int *__restrict__ ucount, int *__restrict__ inpos, int *__restrict__ outpos)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_eq) return;
+    int c = cell[part_of_row[r]];
+    int r0 = cell_row0[c], r1 = r0 + ucount[c];
+    int pd = diagpos[r];
+    int q = pd;
+    while (q > row_ptr[r] && col[q - 1] >= r0) q--;
+    inpos[r] = q;
+    q = pd + 1;
+    int e = row_ptr[r + 1];
+    while (q < e && col[q] < r1) q++;
+    outpos[r] = q;
+}
+
+template <bool FWD>
+__device__ __forceinline__ void sweep_cell(int r0, int m, const int *__restrict__ row_ptr,
+                                           const int *__restrict__ diagpos, const int *__restrict__ inpos,
+                                           const int *__restrict__ outpos, const int *__restrict__ col,
+                                           const double *__restrict__ F, const double *__restrict__ rhs, double *x,
+                                           double *sh)
+{
+    int lane = threadIdx.x & 31;
+    if (m > SWEEP_MAXM) {
+        // row by row (no shared-memory staging)
+        for (int t = 0; t < m; t++) {
+            int r = FWD ? r0 + t : r0 + m - 1 - t;
+            int a = FWD ? row_ptr[r] : diagpos[r] + 1;
+            int b = FWD ? diagpos[r] : row_ptr[r + 1];
+            double part = 0.0;
+            for (int q = a + lane; q < b; q += 32) part += F[q] * x[col[q]];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+            if (lane == 0) x[r] = (rhs[r] - part) * F[diagpos[r]];
+            __syncwarp();
+        }
+        return;
+    }
+    // phase 1: cross-cell runs, 8 lanes per row
+    int sub = lane >> 3, sl = lane & 7;
+    for (int t0 = 0; t0 < m; t0 += 4) {
+        int t = t0 + sub;
+        double part = 0.0;
+        if (t < m) {
+            int r = r0 + t;
+            int a = FWD ? row_ptr[r] : outpos[r];
+            int b = FWD ? inpos[r] : row_ptr[r + 1];
+            for (int q = a + sl; q < b; q += 8) part += F[q] * x[col[q]];
+        }
+        part += __shfl_xor_sync(0xffffffffu, part, 1);
+        part += __shfl_xor_sync(0xffffffffu, part, 2);
+        part += __shfl_xor_sync(0xffffffffu, part, 4);
+        if (sl == 0 && t < m) sh[t] = part;
+    }
+    __syncwarp();
+    // phase 2: in-cell solve, lane-owned rows
+    constexpr int R = SWEEP_MAXM / 32;
+    double acc[R];
+    int cur[R], stop[R];
+    int ccol[R];
+    double cval[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        int t = lane + 32 * j;
+        acc[j] = 0.0;
+        cur[j] = stop[j] = 0;
+        ccol[j] = -1;
+        cval[j] = 0.0;
+        if (t < m) {
+            int r = r0 + t;
+            acc[j] = rhs[r] - sh[t];
+            if (FWD) { cur[j] = inpos[r]; stop[j] = diagpos[r]; }
+            else { cur[j] = outpos[r] - 1; stop[j] = diagpos[r]; }
+            if (cur[j] != stop[j]) { ccol[j] = col[cur[j]]; cval[j] = F[cur[j]]; }
+        }
+    }
+    for (int s = 0; s < m; s++) {
+        int k = FWD ? s : m - 1 - s;
+        int owner = k & 31, slot = k >> 5;
+        double v = 0.0;
+#pragma unroll
+        for (int j = 0; j < R; j++)
+            if (j == slot && lane == owner) {
+                v = acc[j] * F[diagpos[r0 + k]];
+                x[r0 + k] = v;
+            }
+        v = __shfl_sync(0xffffffffu, v, owner);
+        int ck = r0 + k;
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            if (ccol[j] == ck) {
+                acc[j] -= cval[j] * v;
+                cur[j] += FWD ? 1 : -1;
+                if (cur[j] != stop[j]) { ccol[j] = col[cur[j]]; cval[j] = F[cur[j]]; }
+                else ccol[j] = -1;
+            }
+        }
+    }
+    __syncwarp();
+}
 
 // Forward L y = r on the cells of one colour.
-__global__ void k_fwd_color(int kbeg, int kend, const int *__restrict__ ccells, const int *__restrict__ cell_row0,
-                            const int *__restrict__ ucount, const int *__restrict__ row_ptr,
-                            const int *__restrict__ diagpos, const int *__restrict__ col,
-                            const double *__restrict__ F, const double *__restrict__ rhs, double *y,
-                            const CGScalars *sc)
+__global__ void __launch_bounds__(32 * SWEEP_WARPS)
+k_fwd_color(int kbeg, int kend, const int *__restrict__ acells, const int *__restrict__ cell_row0,
+            const int *__restrict__ ucount, const int *__restrict__ row_ptr, const int *__restrict__ diagpos,
+            const int *__restrict__ inpos, const int *__restrict__ outpos, const int *__restrict__ col,
+            const double *__restrict__ F, const double *__restrict__ rhs, double *y, const CGScalars *sc)
 {
+    __shared__ double sh[SWEEP_WARPS][SWEEP_MAXM];
     if (sc->done) return;
-    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
-    int kk = kbeg + warp;
+    int w = threadIdx.x >> 5;
+    int kk = kbeg + blockIdx.x * SWEEP_WARPS + w;
     if (kk >= kend) return;
-    int c = ccells[kk];
-    int r0 = cell_row0[c], m = ucount[c];
-    for (int r = r0; r < r0 + m; r++) {
-        int p0 = row_ptr[r], pd = diagpos[r];
-        double part = 0.0;
-        for (int q = p0 + lane; q < pd; q += 32) part += F[q] * y[col[q]];
-        double s = warp_allsum(part);
-        if (lane == 0) y[r] = (rhs[r] - s) * F[pd];
-        __syncwarp();
-    }
+    int c = acells[kk];
+    sweep_cell<true>(cell_row0[c], ucount[c], row_ptr, diagpos, inpos, outpos, col, F, rhs, y, sh[w]);
 }
 
 // Backward L^T z = y on the cells of one colour (colours in reverse).
-__global__ void k_bwd_color(int kbeg, int kend, const int *__restrict__ ccells, const int *__restrict__ cell_row0,
-                            const int *__restrict__ ucount, const int *__restrict__ row_ptr,
-                            const int *__restrict__ diagpos, const int *__restrict__ col,
-                            const double *__restrict__ F, const double *__restrict__ y, double *z,
-                            const CGScalars *sc)
+__global__ void __launch_bounds__(32 * SWEEP_WARPS)
+k_bwd_color(int kbeg, int kend, const int *__restrict__ acells, const int *__restrict__ cell_row0,
+            const int *__restrict__ ucount, const int *__restrict__ row_ptr, const int *__restrict__ diagpos,
+            const int *__restrict__ inpos, const int *__restrict__ outpos, const int *__restrict__ col,
+            const double *__restrict__ F, const double *__restrict__ y, double *z, const CGScalars *sc)
+{
+    __shared__ double sh[SWEEP_WARPS][SWEEP_MAXM];
+    if (sc->done) return;
+    int w = threadIdx.x >> 5;
+    int kk = kbeg + blockIdx.x * SWEEP_WARPS + w;
+    if (kk >= kend) return;
+    int c = acells[kk];
+    sweep_cell<false>(cell_row0[c], ucount[c], row_ptr, diagpos, inpos, outpos, col, F, y, z, sh[w]);
+}
+
+// ---- split sweeps: cross-cell products, then the in-cell solve -------------
+//
+// k_sweep_cross: every row of a colour (rows [rbeg, rend) are contiguous)
+// sums its cross-cell run against the finished colours, LPR lanes per row,
+// into part[r] = rhs[r] - sum.  k_sweep_cell: a warp per cell stages the
+// cell's in-cell runs (local column index and value) and the diagonal
+// inverses in shared memory, then runs the lane-per-row solve from there.
+
+template <bool FWD, int LPR>
+__global__ void k_sweep_cross(int rbeg, int rend, const int *__restrict__ row_ptr, const int *__restrict__ inpos,
+                              const int *__restrict__ outpos, const int *__restrict__ col,
+                              const double *__restrict__ F, const double *__restrict__ rhs, const double *x,
+                              double *__restrict__ part, const CGScalars *sc)
 {
     if (sc->done) return;
-    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    int lane = threadIdx.x & 31;
-    int kk = kbeg + warp;
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int r = rbeg + t / LPR;
+    int lane = t % LPR;
+    double s = 0.0;
+    if (r < rend) {
+        int a = FWD ? __ldg(&row_ptr[r]) : __ldg(&outpos[r]);
+        int b = FWD ? __ldg(&inpos[r]) : __ldg(&row_ptr[r + 1]);
+#pragma unroll 4
+        for (int q = a + lane; q < b; q += LPR) s += __ldg(&F[q]) * x[__ldg(&col[q])];
+    }
+#pragma unroll
+    for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LPR);
+    if (lane == 0 && r < rend) part[r] = rhs[r] - s;
+}
+
+constexpr int CELL_MAXE = 1536;  // staged in-cell entries per warp
+constexpr int CELL_WARPS = 2;    // warps per block of k_sweep_cell
+
+// Packed in-cell factor, built once per step after the factorisation.  For
+// every row r, lo: its in-cell lower entries in ascending column order
+// (forward walk order), up: its in-cell upper entries in descending column
+// order (backward walk order); entries hold the column's index within the
+// cell and the factor value.  Rows are numbered cell by cell, so a cell's
+// entries form one contiguous block.  dinv[r] = 1 / L_rr.
+__global__ void k_pack_lengths(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ diagpos,
+                               const int *__restrict__ inpos, const int *__restrict__ outpos,
+                               int *__restrict__ len_lo, int *__restrict__ len_up)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_eq) return;
+    int pd = diagpos[r];
+    len_lo[r] = pd - inpos[r];
+    len_up[r] = outpos[r] - pd - 1;
+}
+
+__global__ void k_pack_fill(int n_eq, const int *__restrict__ diagpos, const int *__restrict__ inpos,
+                            const int *__restrict__ outpos, const int *__restrict__ col, const double *__restrict__ F,
+                            const int *__restrict__ part_of_row, const int *__restrict__ cell,
+                            const int *__restrict__ cell_row0, const int *__restrict__ off_lo,
+                            const int *__restrict__ off_up, double *__restrict__ lo_val,
+                            unsigned char *__restrict__ lo_k, double *__restrict__ up_val,
+                            unsigned char *__restrict__ up_k, double *__restrict__ dinv, unsigned *err)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_eq) return;
+    int r0 = cell_row0[cell[part_of_row[r]]];
+    if (r - r0 > 255) atomicOr(err, ERR_CELL_OVERFULL);
+    int pd = diagpos[r];
+    dinv[r] = F[pd];
+    int o = off_lo[r];
+    for (int q = inpos[r]; q < pd; q++, o++) {
+        lo_val[o] = F[q];
+        lo_k[o] = (unsigned char)(col[q] - r0);
+    }
+    o = off_up[r];
+    for (int q = outpos[r] - 1; q > pd; q--, o++) {
+        up_val[o] = F[q];
+        up_k[o] = (unsigned char)(col[q] - r0);
+    }
+}
+
+// (first row, unknowns) of every active cell
+__global__ void k_cell_desc(int nact, const int *__restrict__ acells, const int *__restrict__ cell_row0,
+                            const int *__restrict__ ucount, int2 *__restrict__ desc)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nact) return;
+    int c = acells[k];
+    desc[k] = make_int2(cell_row0[c], ucount[c]);
+}
+
+// In-cell solve of one colour, a warp per cell (see the section comment).
+// part[r] = rhs[r] - cross-cell sum; writes x for the cell's rows.
+template <bool FWD>
+__global__ void __launch_bounds__(32 * CELL_WARPS)
+k_sweep_cell(int kbeg, int kend, const int2 *__restrict__ desc, const int *__restrict__ pk_off,
+             const int *__restrict__ pk_len, const double *__restrict__ pk_val,
+             const unsigned char *__restrict__ pk_k, const double *__restrict__ dinv,
+             const double *__restrict__ part, double *__restrict__ x, const CGScalars *sc)
+{
+    __shared__ double s_val[CELL_WARPS][CELL_MAXE];
+    __shared__ unsigned char s_k[CELL_WARPS][CELL_MAXE];
+    if (sc->done) return;
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int kk = kbeg + blockIdx.x * CELL_WARPS + w;
     if (kk >= kend) return;
-    int c = ccells[kk];
-    int r0 = cell_row0[c], m = ucount[c];
-    for (int r = r0 + m - 1; r >= r0; r--) {
-        int pd = diagpos[r], p1 = row_ptr[r + 1];
-        double part = 0.0;
-        for (int q = pd + 1 + lane; q < p1; q += 32) part += F[q] * z[col[q]];
-        double s = warp_allsum(part);
-        if (lane == 0) z[r] = (y[r] - s) * F[pd];
+    int2 dd = desc[kk];
+    int r0 = dd.x, m = dd.y;
+    if (m > SWEEP_MAXM) {
+        // larger than the lane slots: row by row from the packed runs
+        for (int t = 0; t < m; t++) {
+            int r = FWD ? r0 + t : r0 + m - 1 - t;
+            int o = pk_off[r], l = pk_len[r];
+            double ps = 0.0;
+            for (int e = lane; e < l; e += 32) ps += pk_val[o + e] * x[r0 + pk_k[o + e]];
+#pragma unroll
+            for (int q = 16; q > 0; q >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, q);
+            if (lane == 0) x[r] = (part[r] - ps) * dinv[r];
+            __syncwarp();
+        }
+        return;
+    }
+    constexpr int R = SWEEP_MAXM / 32;
+    int off[R], len[R];
+    double acc[R], dv[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        int t = lane + 32 * j;
+        off[j] = len[j] = 0;
+        acc[j] = dv[j] = 0.0;
+        if (t < m) {
+            int r = r0 + t;
+            off[j] = pk_off[r];
+            len[j] = pk_len[r];
+            acc[j] = part[r];
+            dv[j] = dinv[r];
+        }
+    }
+    int base = __shfl_sync(0xffffffffu, off[0], 0);
+    int endo = 0;
+#pragma unroll
+    for (int j = 0; j < R; j++) endo = max(endo, len[j] > 0 ? off[j] + len[j] : 0);
+#pragma unroll
+    for (int q = 16; q > 0; q >>= 1) endo = max(endo, __shfl_xor_sync(0xffffffffu, endo, q));
+    int total = endo > base ? endo - base : 0;
+    bool staged = total <= CELL_MAXE;
+    if (staged) {
+#pragma unroll 4
+        for (int e = lane; e < total; e += 32) {
+            s_val[w][e] = pk_val[base + e];
+            s_k[w][e] = pk_k[base + e];
+        }
         __syncwarp();
+    }
+    int cur[R], ck[R];
+    double cv[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        cur[j] = 0;
+        ck[j] = -1;
+        cv[j] = 0.0;
+        if (len[j] > 0) {
+            int e = off[j] - base;
+            ck[j] = staged ? s_k[w][e] : pk_k[base + e];
+            cv[j] = staged ? s_val[w][e] : pk_val[base + e];
+        }
+    }
+    for (int sidx = 0; sidx < m; sidx++) {
+        int k = FWD ? sidx : m - 1 - sidx;
+        int owner = k & 31, slot = k >> 5;
+        double v = 0.0;
+#pragma unroll
+        for (int j = 0; j < R; j++)
+            if (j == slot && lane == owner) {
+                v = acc[j] * dv[j];
+                x[r0 + k] = v;
+            }
+        v = __shfl_sync(0xffffffffu, v, owner);
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            if (ck[j] == k) {
+                acc[j] -= cv[j] * v;
+                if (++cur[j] < len[j]) {
+                    int e = off[j] - base + cur[j];
+                    ck[j] = staged ? s_k[w][e] : pk_k[base + e];
+                    cv[j] = staged ? s_val[w][e] : pk_val[base + e];
+                } else {
+                    ck[j] = -1;
+                }
+            }
+        }
     }
 }
 
@@ -376,7 +758,9 @@ __global__ void k_cg_spmv(int n_eq, const int *__restrict__ row_ptr, const int *
         int r = rb + threadIdx.x / LPR;
         double s = 0.0;
         if (r < n_eq) {
-            for (int q = row_ptr[r] + lane; q < row_ptr[r + 1]; q += LPR) s += A[q] * p[col[q]];
+            int q1 = __ldg(&row_ptr[r + 1]);
+#pragma unroll 4
+            for (int q = __ldg(&row_ptr[r]) + lane; q < q1; q += LPR) s += __ldg(&A[q]) * p[__ldg(&col[q])];
         }
 #pragma unroll
         for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LPR);
