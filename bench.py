@@ -170,9 +170,10 @@ def measured_peaks():
 
 
 def ncu_traffic(kernel: str):
-    """Per-launch DRAM bytes of `kernel` from the committed ncu summary
-    (profiles/*.md lines 'traffic_per_launch_bytes <kernel> <bytes> <nnz>'),
-    scaled to this workload's nnz by the bench; None when absent."""
+    """(DRAM bytes per launch, algorithmic bytes per launch) of `kernel` from
+    the committed ncu summary (profiles/*.md lines
+    'traffic_per_launch_bytes <kernel> <dram bytes> <algorithmic bytes>');
+    None when absent.  The bench scales the ratio to its own workload."""
     d = os.path.join(ROOT, "profiles")
     if not os.path.isdir(d):
         return None
@@ -271,7 +272,7 @@ def run_b200(args, rank: int, world: int, local_rank: int):
         tr = ncu_traffic("k_cg_spmv")
         traffic = None
         if tr is not None:
-            traffic = tr[0] / tr[1] * nnz_mean
+            traffic = tr[0] / tr[1] * alg_bytes
         fwd_ms = met["prof_fwd_ms"] / max(met["prof_fwd_sweeps"], 1)
         bwd_ms = met["prof_bwd_ms"] / max(met["prof_bwd_sweeps"], 1)
         cpu = None

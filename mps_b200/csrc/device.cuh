@@ -250,9 +250,9 @@ __device__ __forceinline__ double block_sum(double v, double *sh)
     return r;   // valid in thread 0
 }
 
-// Returns true in exactly one thread of the last block to arrive; that
-// thread then owns partials[0..nblocks).
-__device__ __forceinline__ bool last_block_done(unsigned *ticket, unsigned nblocks)
+// True in every thread of the last block to arrive (which then owns
+// partials[0..nblocks)); the ticket is reset for the next launch.
+__device__ __forceinline__ bool last_block(unsigned *ticket, unsigned nblocks)
 {
     __shared__ bool last;
     __threadfence();
@@ -262,7 +262,7 @@ __device__ __forceinline__ bool last_block_done(unsigned *ticket, unsigned nbloc
         if (last) *ticket = 0u;
     }
     __syncthreads();
-    return last && threadIdx.x == 0;
+    return last;
 }
 
 }  // namespace mps

@@ -36,7 +36,7 @@ namespace mps {
 static inline int nblk(long long n, int b) { return (int)((n + b - 1) / b); }
 
 constexpr int TPB = 256;             // threads per block, particle kernels
-constexpr int RED_BLOCKS = 148 * 4;  // fixed grid of the reduction kernels
+constexpr int RED_BLOCKS = 148 * 8;  // fixed grid of the reduction kernels: full occupancy at 256 threads
 constexpr int CG_BATCH = 8;          // CG iterations between convergence reads
 
 template <int D>
@@ -224,6 +224,7 @@ private:
     int n_eq_ = 0;
     long long nnz_ = 0;
     int spmv_lpr_ = 8;   // lanes per row of the CG SpMV (MPS_SPMV_LPR: 8, 16 or 32)
+    int cross_lpr_ = 8;  // lanes per row of the sweeps' cross-cell products (MPS_CROSS_LPR: 4, 8, 16)
     bool ppe_valid_ = false;
 
     // ---- misc
@@ -281,6 +282,11 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
         int v = std::atoi(e);
         if (v == 8 || v == 16 || v == 32) spmv_lpr_ = v;
     }
+    if (const char *e = std::getenv("MPS_CROSS_LPR")) {
+        int v = std::atoi(e);
+        if (v == 4 || v == 8 || v == 16) cross_lpr_ = v;
+    }
+
     MPS_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
     for (auto &e : ev_) MPS_CUDA(cudaEventCreate(&e));
     for (auto &e : pev_) MPS_CUDA(cudaEventCreate(&e));
@@ -953,36 +959,33 @@ void Engine<D>::ppe(bool clamp)
     double *z = icc ? z_.p : r_.p;
     // IC(0) sweeps, per colour: cross-cell products of all its rows, then the
     // in-cell solve a warp per cell.
-    auto fwd = [&]() {
-        for (int c = 0; c < ncol; c++) {
-            int rb = row_off_[c], re = row_off_[c + 1];
-            if (re <= rb) continue;
-            launch(k_sweep_cross<true, 8>, nblk((long long)(re - rb) * 8, 256), 256, 0, st_, rb, re,
-                   (const int *)row_ptr_.p, (const int *)inpos_.p, (const int *)outpos_.p, (const int *)col_.p,
-                   (const double *)F_.p, (const double *)r_.p, (const double *)y_.p, part_.p,
-                   (const CGScalars *)sc_.p);
+    // IC(0) sweeps per colour: the cross-cell products of all the colour's
+    // rows, then the in-cell solve a warp per cell from staged packed runs.
+    auto sweep = [&](bool fwdir) {
+        const double *rhs = fwdir ? r_.p : y_.p;
+        double *out = fwdir ? y_.p : z_.p;
+        const int *pko = fwdir ? pk_off_lo_.p : pk_off_up_.p, *pkl = fwdir ? pk_len_lo_.p : pk_len_up_.p;
+        const double *pkv = fwdir ? pk_val_lo_.p : pk_val_up_.p;
+        const unsigned char *pkk = fwdir ? pk_k_lo_.p : pk_k_up_.p;
+        for (int i = 0; i < ncol; i++) {
+            int c = fwdir ? i : ncol - 1 - i;
             int kb = act_off_[c], ke = act_off_[c + 1];
-            launch(k_sweep_cell<true>, nblk(ke - kb, CELL_WARPS), 32 * CELL_WARPS, 0, st_, kb, ke,
-                   (const int2 *)adesc_.p, (const int *)pk_off_lo_.p, (const int *)pk_len_lo_.p,
-                   (const double *)pk_val_lo_.p, (const unsigned char *)pk_k_lo_.p, (const double *)dinv_.p,
-                   (const double *)part_.p, y_.p, (const CGScalars *)sc_.p);
+            int rb = row_off_[c], re = row_off_[c + 1];
+            if (ke <= kb) continue;
+            auto crossk = fwdir ? (cross_lpr_ == 4 ? k_sweep_cross<true, 4>
+                                                   : cross_lpr_ == 16 ? k_sweep_cross<true, 16> : k_sweep_cross<true, 8>)
+                                : (cross_lpr_ == 4 ? k_sweep_cross<false, 4>
+                                                   : cross_lpr_ == 16 ? k_sweep_cross<false, 16> : k_sweep_cross<false, 8>);
+            launch(crossk, nblk((long long)(re - rb) * cross_lpr_, 256), 256, 0, st_, rb, re, (const int *)row_ptr_.p,
+                   (const int *)inpos_.p, (const int *)outpos_.p, (const int *)col_.p, (const double *)F_.p, rhs,
+                   (const double *)out, part_.p, (const CGScalars *)sc_.p);
+            auto cellk = fwdir ? k_sweep_cell<true> : k_sweep_cell<false>;
+            launch(cellk, nblk(ke - kb, CELL_WARPS), 32 * CELL_WARPS, 0, st_, kb, ke, (const int2 *)adesc_.p, pko,
+                   pkl, pkv, pkk, (const double *)dinv_.p, (const double *)part_.p, out, (const CGScalars *)sc_.p);
         }
     };
-    auto bwd = [&]() {
-        for (int c = ncol - 1; c >= 0; c--) {
-            int rb = row_off_[c], re = row_off_[c + 1];
-            if (re <= rb) continue;
-            launch(k_sweep_cross<false, 8>, nblk((long long)(re - rb) * 8, 256), 256, 0, st_, rb, re,
-                   (const int *)row_ptr_.p, (const int *)inpos_.p, (const int *)outpos_.p, (const int *)col_.p,
-                   (const double *)F_.p, (const double *)y_.p, (const double *)z_.p, part_.p,
-                   (const CGScalars *)sc_.p);
-            int kb = act_off_[c], ke = act_off_[c + 1];
-            launch(k_sweep_cell<false>, nblk(ke - kb, CELL_WARPS), 32 * CELL_WARPS, 0, st_, kb, ke,
-                   (const int2 *)adesc_.p, (const int *)pk_off_up_.p, (const int *)pk_len_up_.p,
-                   (const double *)pk_val_up_.p, (const unsigned char *)pk_k_up_.p, (const double *)dinv_.p,
-                   (const double *)part_.p, z_.p, (const CGScalars *)sc_.p);
-        }
-    };
+    auto fwd = [&]() { sweep(true); };
+    auto bwd = [&]() { sweep(false); };
     auto spmv = [&](int ne) {
         const int *rp = row_ptr_.p, *ci = col_.p;
         const double *av = A_.p, *pv = p_.p;

@@ -426,124 +426,6 @@ __global__ void k_row_splits(int n_eq, const int *__restrict__ row_ptr, const in
     outpos[r] = q;
 }
 
-template <bool FWD>
-__device__ __forceinline__ void sweep_cell(int r0, int m, const int *__restrict__ row_ptr,
-                                           const int *__restrict__ diagpos, const int *__restrict__ inpos,
-                                           const int *__restrict__ outpos, const int *__restrict__ col,
-                                           const double *__restrict__ F, const double *__restrict__ rhs, double *x,
-                                           double *sh)
-{
-    int lane = threadIdx.x & 31;
-    if (m > SWEEP_MAXM) {
-        // row by row (no shared-memory staging)
-        for (int t = 0; t < m; t++) {
-            int r = FWD ? r0 + t : r0 + m - 1 - t;
-            int a = FWD ? row_ptr[r] : diagpos[r] + 1;
-            int b = FWD ? diagpos[r] : row_ptr[r + 1];
-            double part = 0.0;
-            for (int q = a + lane; q < b; q += 32) part += F[q] * x[col[q]];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-            if (lane == 0) x[r] = (rhs[r] - part) * F[diagpos[r]];
-            __syncwarp();
-        }
-        return;
-    }
-    // phase 1: cross-cell runs, 8 lanes per row
-    int sub = lane >> 3, sl = lane & 7;
-    for (int t0 = 0; t0 < m; t0 += 4) {
-        int t = t0 + sub;
-        double part = 0.0;
-        if (t < m) {
-            int r = r0 + t;
-            int a = FWD ? row_ptr[r] : outpos[r];
-            int b = FWD ? inpos[r] : row_ptr[r + 1];
-            for (int q = a + sl; q < b; q += 8) part += F[q] * x[col[q]];
-        }
-        part += __shfl_xor_sync(0xffffffffu, part, 1);
-        part += __shfl_xor_sync(0xffffffffu, part, 2);
-        part += __shfl_xor_sync(0xffffffffu, part, 4);
-        if (sl == 0 && t < m) sh[t] = part;
-    }
-    __syncwarp();
-    // phase 2: in-cell solve, lane-owned rows
-    constexpr int R = SWEEP_MAXM / 32;
-    double acc[R];
-    int cur[R], stop[R];
-    int ccol[R];
-    double cval[R];
-#pragma unroll
-    for (int j = 0; j < R; j++) {
-        int t = lane + 32 * j;
-        acc[j] = 0.0;
-        cur[j] = stop[j] = 0;
-        ccol[j] = -1;
-        cval[j] = 0.0;
-        if (t < m) {
-            int r = r0 + t;
-            acc[j] = rhs[r] - sh[t];
-            if (FWD) { cur[j] = inpos[r]; stop[j] = diagpos[r]; }
-            else { cur[j] = outpos[r] - 1; stop[j] = diagpos[r]; }
-            if (cur[j] != stop[j]) { ccol[j] = col[cur[j]]; cval[j] = F[cur[j]]; }
-        }
-    }
-    for (int s = 0; s < m; s++) {
-        int k = FWD ? s : m - 1 - s;
-        int owner = k & 31, slot = k >> 5;
-        double v = 0.0;
-#pragma unroll
-        for (int j = 0; j < R; j++)
-            if (j == slot && lane == owner) {
-                v = acc[j] * F[diagpos[r0 + k]];
-                x[r0 + k] = v;
-            }
-        v = __shfl_sync(0xffffffffu, v, owner);
-        int ck = r0 + k;
-#pragma unroll
-        for (int j = 0; j < R; j++) {
-            if (ccol[j] == ck) {
-                acc[j] -= cval[j] * v;
-                cur[j] += FWD ? 1 : -1;
-                if (cur[j] != stop[j]) { ccol[j] = col[cur[j]]; cval[j] = F[cur[j]]; }
-                else ccol[j] = -1;
-            }
-        }
-    }
-    __syncwarp();
-}
-
-// Forward L y = r on the cells of one colour.
-__global__ void __launch_bounds__(32 * SWEEP_WARPS)
-k_fwd_color(int kbeg, int kend, const int *__restrict__ acells, const int *__restrict__ cell_row0,
-            const int *__restrict__ ucount, const int *__restrict__ row_ptr, const int *__restrict__ diagpos,
-            const int *__restrict__ inpos, const int *__restrict__ outpos, const int *__restrict__ col,
-            const double *__restrict__ F, const double *__restrict__ rhs, double *y, const CGScalars *sc)
-{
-    __shared__ double sh[SWEEP_WARPS][SWEEP_MAXM];
-    if (sc->done) return;
-    int w = threadIdx.x >> 5;
-    int kk = kbeg + blockIdx.x * SWEEP_WARPS + w;
-    if (kk >= kend) return;
-    int c = acells[kk];
-    sweep_cell<true>(cell_row0[c], ucount[c], row_ptr, diagpos, inpos, outpos, col, F, rhs, y, sh[w]);
-}
-
-// Backward L^T z = y on the cells of one colour (colours in reverse).
-__global__ void __launch_bounds__(32 * SWEEP_WARPS)
-k_bwd_color(int kbeg, int kend, const int *__restrict__ acells, const int *__restrict__ cell_row0,
-            const int *__restrict__ ucount, const int *__restrict__ row_ptr, const int *__restrict__ diagpos,
-            const int *__restrict__ inpos, const int *__restrict__ outpos, const int *__restrict__ col,
-            const double *__restrict__ F, const double *__restrict__ y, double *z, const CGScalars *sc)
-{
-    __shared__ double sh[SWEEP_WARPS][SWEEP_MAXM];
-    if (sc->done) return;
-    int w = threadIdx.x >> 5;
-    int kk = kbeg + blockIdx.x * SWEEP_WARPS + w;
-    if (kk >= kend) return;
-    int c = acells[kk];
-    sweep_cell<false>(cell_row0[c], ucount[c], row_ptr, diagpos, inpos, outpos, col, F, y, z, sh[w]);
-}
-
 // ---- split sweeps: cross-cell products, then the in-cell solve -------------
 //
 // k_sweep_cross: every row of a colour (rows [rbeg, rend) are contiguous)
@@ -574,7 +456,7 @@ __global__ void k_sweep_cross(int rbeg, int rend, const int *__restrict__ row_pt
     if (lane == 0 && r < rend) part[r] = rhs[r] - s;
 }
 
-constexpr int CELL_MAXE = 1536;  // staged in-cell entries per warp
+constexpr int CELL_MAXE = 1536;  // staged in-cell entries per warp (larger cells read the packed runs directly)
 constexpr int CELL_WARPS = 2;    // warps per block of k_sweep_cell
 
 // Packed in-cell factor, built once per step after the factorisation.  For
@@ -628,6 +510,55 @@ __global__ void k_cell_desc(int nact, const int *__restrict__ acells, const int 
     if (k >= nact) return;
     int c = acells[k];
     desc[k] = make_int2(cell_row0[c], ucount[c]);
+}
+
+// Lane-per-row solve of one cell from a staged entry block (lo/up runs in
+// walk order, local column index in `ks`).  R = row slots per lane.
+template <bool FWD, int R>
+__device__ __forceinline__ void cell_solve(int r0, int m, const int *off, const int *len, double *acc,
+                                           const double *dv, const double *vals, const unsigned char *ks,
+                                           double *__restrict__ x)
+{
+    int lane = threadIdx.x & 31;
+    int cur[R], ck[R];
+    double cv[R];
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+        cur[j] = off[j];
+        int end = off[j] + len[j];
+        ck[j] = (cur[j] < end) ? (int)ks[cur[j]] : -1;
+        cv[j] = (cur[j] < end) ? vals[cur[j]] : 0.0;
+    }
+    for (int sidx = 0; sidx < m; sidx++) {
+        int k = FWD ? sidx : m - 1 - sidx;
+        int owner = k & 31;
+        double v = 0.0;
+        if (R == 1) {
+            if (lane == owner) {
+                v = acc[0] * dv[0];
+                x[r0 + k] = v;
+            }
+        } else {
+            int slot = k >> 5;
+#pragma unroll
+            for (int j = 0; j < R; j++)
+                if (j == slot && lane == owner) {
+                    v = acc[j] * dv[j];
+                    x[r0 + k] = v;
+                }
+        }
+        v = __shfl_sync(0xffffffffu, v, owner);
+#pragma unroll
+        for (int j = 0; j < R; j++) {
+            if (ck[j] == k) {
+                acc[j] -= cv[j] * v;
+                ++cur[j];
+                bool more = cur[j] < off[j] + len[j];
+                ck[j] = more ? (int)ks[cur[j]] : -1;
+                cv[j] = more ? vals[cur[j]] : 0.0;
+            }
+        }
+    }
 }
 
 // In-cell solve of one colour, a warp per cell (see the section comment).
@@ -684,58 +615,41 @@ k_sweep_cell(int kbeg, int kend, const int2 *__restrict__ desc, const int *__res
 #pragma unroll
     for (int q = 16; q > 0; q >>= 1) endo = max(endo, __shfl_xor_sync(0xffffffffu, endo, q));
     int total = endo > base ? endo - base : 0;
-    bool staged = total <= CELL_MAXE;
-    if (staged) {
+    const double *vals;
+    const unsigned char *ks;
+    if (total <= CELL_MAXE) {
 #pragma unroll 4
         for (int e = lane; e < total; e += 32) {
             s_val[w][e] = pk_val[base + e];
             s_k[w][e] = pk_k[base + e];
         }
         __syncwarp();
-    }
-    int cur[R], ck[R];
-    double cv[R];
 #pragma unroll
-    for (int j = 0; j < R; j++) {
-        cur[j] = 0;
-        ck[j] = -1;
-        cv[j] = 0.0;
-        if (len[j] > 0) {
-            int e = off[j] - base;
-            ck[j] = staged ? s_k[w][e] : pk_k[base + e];
-            cv[j] = staged ? s_val[w][e] : pk_val[base + e];
-        }
+        for (int j = 0; j < R; j++) off[j] -= base;
+        vals = s_val[w];
+        ks = s_k[w];
+    } else {
+        vals = pk_val;
+        ks = pk_k;
     }
-    for (int sidx = 0; sidx < m; sidx++) {
-        int k = FWD ? sidx : m - 1 - sidx;
-        int owner = k & 31, slot = k >> 5;
-        double v = 0.0;
-#pragma unroll
-        for (int j = 0; j < R; j++)
-            if (j == slot && lane == owner) {
-                v = acc[j] * dv[j];
-                x[r0 + k] = v;
-            }
-        v = __shfl_sync(0xffffffffu, v, owner);
-#pragma unroll
-        for (int j = 0; j < R; j++) {
-            if (ck[j] == k) {
-                acc[j] -= cv[j] * v;
-                if (++cur[j] < len[j]) {
-                    int e = off[j] - base + cur[j];
-                    ck[j] = staged ? s_k[w][e] : pk_k[base + e];
-                    cv[j] = staged ? s_val[w][e] : pk_val[base + e];
-                } else {
-                    ck[j] = -1;
-                }
-            }
-        }
-    }
+    if (m <= 32) cell_solve<FWD, 1>(r0, m, off, len, acc, dv, vals, ks, x);
+    else if (m <= 64) cell_solve<FWD, 2>(r0, m, off, len, acc, dv, vals, ks, x);
+    else cell_solve<FWD, 4>(r0, m, off, len, acc, dv, vals, ks, x);
 }
 
 // ---- CG vector kernels ------------------------------------------------------
 
 constexpr int CG_BLOCK = 256;
+
+// Sum of partials[0..n) (stride `stride`, offset `o`) by the whole last
+// block: thread t adds slots t, t+CG_BLOCK, ... in order, then a fixed
+// tree; the result (valid in thread 0) is the same on every run.
+__device__ __forceinline__ double final_sum(const double *partials, unsigned n, int stride, int o, double *sh)
+{
+    double a = 0.0;
+    for (unsigned b = threadIdx.x; b < n; b += CG_BLOCK) a += __ldcg(&partials[(size_t)b * stride + o]);
+    return block_sum<CG_BLOCK>(a, sh);
+}
 
 // Ap = A p and the p.Ap partial; the last block forms alpha.  The kernel
 // also performs the loop-head test of the reference (sqrt(r.r) < tol, and
@@ -771,12 +685,13 @@ __global__ void k_cg_spmv(int n_eq, const int *__restrict__ row_ptr, const int *
     }
     double t = block_sum<CG_BLOCK>(acc, sh);
     if (threadIdx.x == 0) partials[blockIdx.x] = t;
-    if (last_block_done(ticket, gridDim.x)) {
-        double tot = 0.0;
-        for (unsigned b = 0; b < gridDim.x; b++) tot += __ldcg(&partials[b]);
-        sc->pAp = tot;
-        if (fabs(tot) < 1.0e-30) { sc->done = 1; sc->breakdown = 1; }
-        else sc->alpha = sc->rz / tot;
+    if (last_block(ticket, gridDim.x)) {
+        double tot = final_sum(partials, gridDim.x, 1, 0, sh);
+        if (threadIdx.x == 0) {
+            sc->pAp = tot;
+            if (fabs(tot) < 1.0e-30) { sc->done = 1; sc->breakdown = 1; }
+            else sc->alpha = sc->rz / tot;
+        }
     }
 }
 
@@ -796,10 +711,9 @@ __global__ void k_cg_axpy(int n_eq, double *__restrict__ x, double *__restrict__
     }
     double t = block_sum<CG_BLOCK>(acc, sh);
     if (threadIdx.x == 0) partials[blockIdx.x] = t;
-    if (last_block_done(ticket, gridDim.x)) {
-        double tot = 0.0;
-        for (unsigned b = 0; b < gridDim.x; b++) tot += __ldcg(&partials[b]);
-        sc->rr = tot;
+    if (last_block(ticket, gridDim.x)) {
+        double tot = final_sum(partials, gridDim.x, 1, 0, sh);
+        if (threadIdx.x == 0) sc->rr = tot;
     }
 }
 
@@ -814,12 +728,13 @@ __global__ void k_cg_rz(int n_eq, const double *__restrict__ r, const double *__
         acc += r[i] * z[i];
     double t = block_sum<CG_BLOCK>(acc, sh);
     if (threadIdx.x == 0) partials[blockIdx.x] = t;
-    if (last_block_done(ticket, gridDim.x)) {
-        double tot = 0.0;
-        for (unsigned b = 0; b < gridDim.x; b++) tot += __ldcg(&partials[b]);
-        sc->rz_new = tot;
-        if (fabs(sc->rz) < 1.0e-60) { sc->done = 1; sc->breakdown = 1; }
-        else { sc->beta = tot / sc->rz; sc->rz = tot; }
+    if (last_block(ticket, gridDim.x)) {
+        double tot = final_sum(partials, gridDim.x, 1, 0, sh);
+        if (threadIdx.x == 0) {
+            sc->rz_new = tot;
+            if (fabs(sc->rz) < 1.0e-60) { sc->done = 1; sc->breakdown = 1; }
+            else { sc->beta = tot / sc->rz; sc->rz = tot; }
+        }
     }
 }
 
@@ -859,17 +774,16 @@ __global__ void k_cg_init2(int n_eq, const double *__restrict__ r, const double 
         partials[2 * blockIdx.x] = ta;
         partials[2 * blockIdx.x + 1] = tb;
     }
-    if (last_block_done(ticket, gridDim.x)) {
-        double sa = 0.0, sb = 0.0;
-        for (unsigned k = 0; k < gridDim.x; k++) {
-            sa += __ldcg(&partials[2 * k]);
-            sb += __ldcg(&partials[2 * k + 1]);
+    if (last_block(ticket, gridDim.x)) {
+        double sa = final_sum(partials, gridDim.x, 2, 0, sh);
+        double sb = final_sum(partials, gridDim.x, 2, 1, sh);
+        if (threadIdx.x == 0) {
+            sc->rz = sa;
+            sc->rr = sb;
+            sc->iter = 0;
+            sc->done = 0;
+            sc->breakdown = 0;
         }
-        sc->rz = sa;
-        sc->rr = sb;
-        sc->iter = 0;
-        sc->done = 0;
-        sc->breakdown = 0;
     }
 }
 
