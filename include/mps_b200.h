@@ -204,6 +204,42 @@ void *mps_get_stream(mps_session *s);
 int  mps_run_stage(mps_session *s, int stage, const int *neighbors, const int *count,
                    int max_nb, double arg);
 
+/* ---- cell sort without device allocation ------------------------------
+ *
+ * No counterpart in the reference (its cell list is host memory allocated
+ * by cell_list_create).  For callers that cannot allocate device memory
+ * where they need the neighbour structure -- a frozen memory pool, a
+ * replayed graph whose addresses must not change, a host program that owns
+ * every buffer -- this sorts particles into the reference's cell grid using
+ * only the caller's arrays plus one static device array of the library
+ * (about 4 MB on every GPU that loads it, held until exit).
+ *
+ * pos: num*dim doubles, particle-major; type: num ints (ghosts are not
+ * binned); all pointers are device memory.  Outputs: cell[num] (the
+ * reference's cell index, -1 if not binned), cell_start[total_cells + 1]
+ * (first slot of each cell; cell_start[total_cells] = binned particles) and
+ * order[num] (particle indices, cell by cell, descending index within a
+ * cell as the reference's chains, then the unbinned ones ascending).
+ * Work is queued on `stream` (a cudaStream_t, 0 = default).
+ *
+ * Limits: num <= MPS_NOALLOC_MAX_PARTICLES, total cells <=
+ * MPS_NOALLOC_MAX_CELLS; larger requests return MPS_ERR_INVALID.  The first
+ * call on a device looks up the static array's device address and should
+ * come before any stream capture.  All calls share that array: calls whose
+ * work overlaps on the GPU race on it and must be ordered by the caller. */
+#define MPS_NOALLOC_MAX_PARTICLES 262144
+#define MPS_NOALLOC_MAX_CELLS     262144
+
+typedef struct {
+    int    dim;          /* 2 or 3 */
+    double origin[3];    /* cell grid origin (cell_list_create: domain_min - 4 re) */
+    double cell_size;    /* re */
+    int    dims[3];      /* cells per axis */
+} mps_grid_t;
+
+int  mps_cell_sort_noalloc(const mps_grid_t *grid, const double *pos, const int *type, int num,
+                           int *cell, int *order, int *cell_start, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -74,6 +74,15 @@ class MpsParams(C.Structure):
     ]
 
 
+class MpsGrid(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int),
+        ("origin", C.c_double * 3),
+        ("cell_size", C.c_double),
+        ("dims", C.c_int * 3),
+    ]
+
+
 class MpsMetrics(C.Structure):
     _fields_ = [
         ("ppe_iterations", C.c_int),
@@ -134,6 +143,7 @@ SIGNATURES = {
     "mps_set_profiling": (I, [P, I]),
     "mps_reset_metrics": (I, [P]),
     "mps_run_stage": (I, [P, I, P, P, I, C.c_double]),
+    "mps_cell_sort_noalloc": (I, [C.POINTER(MpsGrid), P, P, I, P, P, P, P]),
 }
 
 _lib = None

@@ -22,7 +22,7 @@ FLAGS = ["-lineinfo", "-O3", "--fmad=false", "-std=c++17", "-Xcompiler", "-fPIC"
          "-Xcompiler", "-ffp-contract=off"]
 
 TARGETS = {
-    "libmps_b200.so": ["engine.cu"],
+    "libmps_b200.so": ["engine.cu", "noalloc.cu"],
 }
 CXX = os.environ.get("MPS_CXX", "g++")
 CC = os.environ.get("MPS_CC", "gcc")
