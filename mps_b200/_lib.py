@@ -174,7 +174,7 @@ class MpsError(RuntimeError):
         super().__init__(f"{ERRORS.get(code, code)}: {what}")
 
 
-def params_from_config(cfg, dim: int, precision: int = PREC_FP64, refine_tolerance: float = 1e-4) -> MpsParams:
+def params_from_config(cfg, dim: int, precision: int = PREC_FP64, refine_tolerance: float = 1e-10) -> MpsParams:
     """The session parameters of a reference ``SimConfig`` (already parsed)."""
     p = MpsParams()
     p.dim = dim

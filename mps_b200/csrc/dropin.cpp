@@ -95,7 +95,7 @@ mps_params_t params_from(const SimConfig *c)
     p.use_analytical_lambda = c->use_analytical_lambda;
     p.hs_mode = c->hs_mode;
     p.precision = MPS_PREC_FP64;
-    p.refine_tolerance = 1e-4;
+    p.refine_tolerance = 1e-10;
     return p;
 }
 

@@ -216,9 +216,11 @@ private:
     DevArray<unsigned char> pk_k_lo_, pk_k_up_;
     DevArray<int2> adesc_;
 
+
     // ---- PPE
     DevArray<int> ucount_, ucol_, rs_, cell_row0_, row_of_, part_of_row_, rcount_, row_ptr_, diagpos_, col_;
     DevArray<double> A_, F_, b_, x_, r_, z_, p_, Ap_, y_, part_, partials_;
+    DevArray<float> A32_, F32_, pkv32_lo_, pkv32_up_, dinv32_, r32_, z32_, p32_, Ap32_, y32_, part32_, d32_;
     DevArray<CGScalars> sc_;
     DevArray<unsigned> ticket_, err_;
     int n_eq_ = 0;
@@ -256,6 +258,17 @@ private:
     void sort();
     void unsort();
     void ppe(bool clamp);
+    template <class T>
+    struct PcgBufs {
+        const T *A, *F, *pkv_lo, *pkv_up, *dinv;
+        T *x, *r, *z, *p, *Ap, *y, *part;
+        const T *b;
+    };
+    template <class T>
+    void pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, int n_eq, long long nnz);
+    void mixed_solve(int n_eq, long long nnz, bool icc);
+    static constexpr int kMaxOuter = 20;         // refinement sweeps of the mixed form
+    static constexpr double kInnerRtol = 1.0e-5; // FP32 inner solve: residual reduction per sweep
     int read_int(const int *dev);
     void check_err();
     void upload_list(const int *nb, const int *cnt, int max_nb);
@@ -326,6 +339,7 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
     }
     if (D == 3) MPS_CUDA(cudaMemcpyToSymbol(c_order3, t3, sizeof(t3)));
     else MPS_CUDA(cudaMemcpyToSymbol(c_order2, t2, sizeof(t2)));
+
 }
 
 template <int D>
@@ -436,6 +450,7 @@ void Engine<D>::build_grid()
     apos_.reserve(total + 1);
     acells_.reserve(total + 1);
     sizes_.reserve(16);
+
 }
 
 // Constants evaluated with the reference's expressions.
@@ -949,71 +964,95 @@ void Engine<D>::ppe(bool clamp)
     }
     MPS_CUDA(cudaEventRecord(ev_[3], st_));
 
-    // PCG (pressure_solver.c:261-322); CG when solver_type == 0 (:90-131).
-    CGScalars init{};
-    init.tol = prm_.cg_tolerance;
-    init.maxit = prm_.cg_max_iter;
-    MPS_CUDA(cudaMemcpyAsync(sc_.p, &init, sizeof(CGScalars), cudaMemcpyHostToDevice, st_));
+    if (prm_.precision == MPS_PREC_MIXED) {
+        mixed_solve(n_eq, nnz, icc);
+    } else {
+        PcgBufs<double> v{A_.p, F_.p, pk_val_lo_.p, pk_val_up_.p, dinv_.p, x_.p, r_.p, z_.p, p_.p, Ap_.p, y_.p,
+                          part_.p, b_.p};
+        pcg_solve<double>(v, prm_.cg_tolerance, prm_.cg_max_iter, icc, n_eq, nnz);
+        met.ppe_iterations = sc_host_->iter;
+        met.ppe_outer = 1;
+        met.ppe_residual = std::sqrt(sc_host_->rr);
+        met.converged = std::sqrt(sc_host_->rr) < prm_.cg_tolerance;
+        met.total_iterations += sc_host_->iter;
+    }
+    launch(k_writeback<D>, nb, TPB, 0, st_, s, row_of_.p, x_.p, n, clamp);
+    MPS_CUDA(cudaGetLastError());
+    ppe_valid_ = true;
+}
+
+// PCG of pressure_solver.c:261-322 (CG of :90-131 when icc is false) on the
+// block-colour system, values and vectors of type T, dot products in FP64.
+// r is initialised from v.b (which may alias r); stops at sqrt(r.r) < tol,
+// the reference's test, or after maxit iterations.  Leaves the final
+// scalars in *sc_host_.
+template <int D>
+template <class T>
+void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, int n_eq, long long nnz)
+{
+    int ncol = 1 << D;
     const int RB = RED_BLOCKS;
-    launch(k_cg_init, RB, CG_BLOCK, 0, st_, n_eq, x_.p, r_.p, b_.p);
-    double *z = icc ? z_.p : r_.p;
-    // IC(0) sweeps, per colour: cross-cell products of all its rows, then the
-    // in-cell solve a warp per cell.
+    CGScalars init{};
+    init.tol = tol;
+    init.maxit = maxit;
+    MPS_CUDA(cudaMemcpyAsync(sc_.p, &init, sizeof(CGScalars), cudaMemcpyHostToDevice, st_));
+    launch(k_cg_init<T>, RB, CG_BLOCK, 0, st_, n_eq, v.x, v.r, v.b);
+    T *z = icc ? v.z : v.r;
     // IC(0) sweeps per colour: the cross-cell products of all the colour's
     // rows, then the in-cell solve a warp per cell from staged packed runs.
     auto sweep = [&](bool fwdir) {
-        const double *rhs = fwdir ? r_.p : y_.p;
-        double *out = fwdir ? y_.p : z_.p;
+        const T *rhs = fwdir ? v.r : v.y;
+        T *out = fwdir ? v.y : v.z;
         const int *pko = fwdir ? pk_off_lo_.p : pk_off_up_.p, *pkl = fwdir ? pk_len_lo_.p : pk_len_up_.p;
-        const double *pkv = fwdir ? pk_val_lo_.p : pk_val_up_.p;
+        const T *pkv = fwdir ? v.pkv_lo : v.pkv_up;
         const unsigned char *pkk = fwdir ? pk_k_lo_.p : pk_k_up_.p;
         for (int i = 0; i < ncol; i++) {
             int c = fwdir ? i : ncol - 1 - i;
             int kb = act_off_[c], ke = act_off_[c + 1];
             int rb = row_off_[c], re = row_off_[c + 1];
             if (ke <= kb) continue;
-            auto crossk = fwdir ? (cross_lpr_ == 4 ? k_sweep_cross<true, 4>
-                                                   : cross_lpr_ == 16 ? k_sweep_cross<true, 16> : k_sweep_cross<true, 8>)
-                                : (cross_lpr_ == 4 ? k_sweep_cross<false, 4>
-                                                   : cross_lpr_ == 16 ? k_sweep_cross<false, 16> : k_sweep_cross<false, 8>);
-            launch(crossk, nblk((long long)(re - rb) * cross_lpr_, 256), 256, 0, st_, rb, re, (const int *)row_ptr_.p,
-                   (const int *)inpos_.p, (const int *)outpos_.p, (const int *)col_.p, (const double *)F_.p, rhs,
-                   (const double *)out, part_.p, (const CGScalars *)sc_.p);
-            auto cellk = fwdir ? k_sweep_cell<true> : k_sweep_cell<false>;
+            auto crossk = fwdir ? k_sweep_cross<true, 8, T> : k_sweep_cross<false, 8, T>;
+            launch(crossk, nblk((long long)(re - rb) * 8, 256), 256, 0, st_, rb, re, (const int *)row_ptr_.p,
+                   (const int *)inpos_.p, (const int *)outpos_.p, (const int *)col_.p, v.F, rhs, (const T *)out,
+                   v.part, (const CGScalars *)sc_.p);
+            auto cellk = fwdir ? k_sweep_cell<true, T> : k_sweep_cell<false, T>;
             launch(cellk, nblk(ke - kb, CELL_WARPS), 32 * CELL_WARPS, 0, st_, kb, ke, (const int2 *)adesc_.p, pko,
-                   pkl, pkv, pkk, (const double *)dinv_.p, (const double *)part_.p, out, (const CGScalars *)sc_.p);
+                   pkl, pkv, pkk, v.dinv, (const T *)v.part, out, (const CGScalars *)sc_.p);
         }
     };
-    auto fwd = [&]() { sweep(true); };
-    auto bwd = [&]() { sweep(false); };
-    auto spmv = [&](int ne) {
+    auto spmv = [&]() {
         const int *rp = row_ptr_.p, *ci = col_.p;
-        const double *av = A_.p, *pv = p_.p;
-        if (spmv_lpr_ == 8)
-            launch(k_cg_spmv<8>, RB, CG_BLOCK, 0, st_, ne, rp, ci, av, pv, Ap_.p, partials_.p, ticket_.p, sc_.p);
-        else if (spmv_lpr_ == 16)
-            launch(k_cg_spmv<16>, RB, CG_BLOCK, 0, st_, ne, rp, ci, av, pv, Ap_.p, partials_.p, ticket_.p, sc_.p);
+        if (spmv_lpr_ == 16)
+            launch(k_cg_spmv<16, T>, RB, CG_BLOCK, 0, st_, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
+                   ticket_.p, sc_.p);
+        else if (spmv_lpr_ == 32)
+            launch(k_cg_spmv<32, T>, RB, CG_BLOCK, 0, st_, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
+                   ticket_.p, sc_.p);
         else
-            launch(k_cg_spmv<32>, RB, CG_BLOCK, 0, st_, ne, rp, ci, av, pv, Ap_.p, partials_.p, ticket_.p, sc_.p);
+            launch(k_cg_spmv<8, T>, RB, CG_BLOCK, 0, st_, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
+                   ticket_.p, sc_.p);
     };
-    if (icc) { fwd(); bwd(); }
-    launch(k_cg_init2, RB, CG_BLOCK, 0, st_, n_eq, r_.p, z, p_.p, partials_.p, ticket_.p, sc_.p);
+    if (icc) { sweep(true); sweep(false); }
+    launch(k_cg_init2<T>, RB, CG_BLOCK, 0, st_, n_eq, (const T *)v.r, (const T *)z, v.p, partials_.p, ticket_.p,
+           sc_.p);
     int iter_before = 0;
     for (;;) {
         bool prof = profiling;
         for (int it = 0; it < CG_BATCH; it++) {
             cudaEvent_t *e = pev_ + it * PEV;
             if (prof) MPS_CUDA(cudaEventRecord(e[0], st_));
-            spmv(n_eq);
+            spmv();
             if (prof) MPS_CUDA(cudaEventRecord(e[1], st_));
-            launch(k_cg_axpy, RB, CG_BLOCK, 0, st_, n_eq, x_.p, r_.p, p_.p, Ap_.p, partials_.p, ticket_.p, sc_.p);
+            launch(k_cg_axpy<T>, RB, CG_BLOCK, 0, st_, n_eq, v.x, v.r, (const T *)v.p, (const T *)v.Ap, partials_.p,
+                   ticket_.p, sc_.p);
             if (prof) MPS_CUDA(cudaEventRecord(e[2], st_));
-            if (icc) fwd();
+            if (icc) sweep(true);
             if (prof) MPS_CUDA(cudaEventRecord(e[3], st_));
-            if (icc) bwd();
+            if (icc) sweep(false);
             if (prof) MPS_CUDA(cudaEventRecord(e[4], st_));
-            launch(k_cg_rz, RB, CG_BLOCK, 0, st_, n_eq, r_.p, z, partials_.p, ticket_.p, sc_.p);
-            launch(k_cg_update_p, RB, CG_BLOCK, 0, st_, n_eq, p_.p, z, sc_.p);
+            launch(k_cg_rz<T>, RB, CG_BLOCK, 0, st_, n_eq, (const T *)v.r, (const T *)z, partials_.p, ticket_.p,
+                   sc_.p);
+            launch(k_cg_update_p<T>, RB, CG_BLOCK, 0, st_, n_eq, v.p, (const T *)z, sc_.p);
         }
         MPS_CUDA(cudaGetLastError());
         MPS_CUDA(cudaMemcpyAsync(sc_host_, sc_.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, st_));
@@ -1044,14 +1083,56 @@ void Engine<D>::ppe(bool clamp)
         iter_before = sc_host_->iter;
         if (sc_host_->done) break;
     }
-    met.ppe_iterations = sc_host_->iter;
-    met.ppe_outer = 1;
-    met.ppe_residual = std::sqrt(sc_host_->rr);
-    met.converged = std::sqrt(sc_host_->rr) < prm_.cg_tolerance;
-    met.total_iterations += sc_host_->iter;
-    launch(k_writeback<D>, nb, TPB, 0, st_, s, row_of_.p, x_.p, n, clamp);
-    MPS_CUDA(cudaGetLastError());
-    ppe_valid_ = true;
+}
+
+// Mixed form: FP32 inner ICCG on A rounded to FP32 and the FP32-rounded
+// factor, corrected by FP64 iterative refinement, r = b - A x with the FP64
+// A and x, until ||r|| <= max(cg_tolerance, refine_tolerance * ||b||).
+template <int D>
+void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
+{
+    const int RB = RED_BLOCKS;
+    size_t nz = (size_t)nnz;
+    for (auto *v : {&A32_, &F32_, &pkv32_lo_, &pkv32_up_}) v->reserve(nz);
+    for (auto *v : {&dinv32_, &r32_, &z32_, &p32_, &Ap32_, &y32_, &part32_, &d32_}) v->reserve((size_t)cap_);
+    launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)A_.p, A32_.p);
+    if (icc) {
+        launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)F_.p, F32_.p);
+        launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)pk_val_lo_.p, pkv32_lo_.p);
+        launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)pk_val_up_.p, pkv32_up_.p);
+        launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, (size_t)n_eq, (const double *)dinv_.p, dinv32_.p);
+    }
+    CGScalars init{};
+    MPS_CUDA(cudaMemcpyAsync(sc_.p, &init, sizeof(CGScalars), cudaMemcpyHostToDevice, st_));
+    launch(k_refine_init, RB, CG_BLOCK, 0, st_, n_eq, x_.p, r_.p, r32_.p, (const double *)b_.p, partials_.p,
+           ticket_.p, sc_.p);
+    MPS_CUDA(cudaMemcpyAsync(sc_host_, sc_.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+    double bnorm = std::sqrt(sc_host_->rr_outer);
+    double rtol = prm_.refine_tolerance > 0.0 ? prm_.refine_tolerance : 1.0e-10;
+    double target = std::max(prm_.cg_tolerance, rtol * bnorm);
+    double rnorm = bnorm;
+    int outer = 0, inner_total = 0;
+    const int inner_max = std::min(prm_.cg_max_iter, 2000);
+    PcgBufs<float> v{A32_.p, F32_.p, pkv32_lo_.p, pkv32_up_.p, dinv32_.p, d32_.p, r32_.p, z32_.p, p32_.p, Ap32_.p,
+                     y32_.p, part32_.p, r32_.p};
+    while (rnorm > target && outer < kMaxOuter) {
+        pcg_solve<float>(v, kInnerRtol * rnorm, inner_max, icc, n_eq, nnz);
+        inner_total += sc_host_->iter;
+        launch(k_refine_update, RB, CG_BLOCK, 0, st_, n_eq, x_.p, (const float *)d32_.p);
+        launch(k_refine_residual, RB, CG_BLOCK, 0, st_, n_eq, (const int *)row_ptr_.p, (const int *)col_.p,
+               (const double *)A_.p, (const double *)x_.p, (const double *)b_.p, r_.p, r32_.p, partials_.p,
+               ticket_.p, sc_.p);
+        MPS_CUDA(cudaMemcpyAsync(sc_host_, sc_.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, st_));
+        MPS_CUDA(cudaStreamSynchronize(st_));
+        rnorm = std::sqrt(sc_host_->rr_outer);
+        outer++;
+    }
+    met.ppe_iterations = inner_total;
+    met.ppe_outer = outer;
+    met.ppe_residual = rnorm;
+    met.converged = rnorm <= target;
+    met.total_iterations += inner_total;
 }
 
 // ---- introspection --------------------------------------------------------

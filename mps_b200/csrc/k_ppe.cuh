@@ -26,6 +26,7 @@ namespace mps {
 struct CGScalars {
     double rz, rr, pAp, alpha, beta, rz_new;
     double tol;
+    double rr_outer;        // ||b - A x||^2 of the FP64 refinement (mixed form)
     int iter, done, maxit, breakdown;
 };
 
@@ -434,17 +435,17 @@ __global__ void k_row_splits(int n_eq, const int *__restrict__ row_ptr, const in
 // cell's in-cell runs (local column index and value) and the diagonal
 // inverses in shared memory, then runs the lane-per-row solve from there.
 
-template <bool FWD, int LPR>
+template <bool FWD, int LPR, class T>
 __global__ void k_sweep_cross(int rbeg, int rend, const int *__restrict__ row_ptr, const int *__restrict__ inpos,
                               const int *__restrict__ outpos, const int *__restrict__ col,
-                              const double *__restrict__ F, const double *__restrict__ rhs, const double *x,
-                              double *__restrict__ part, const CGScalars *sc)
+                              const T *__restrict__ F, const T *__restrict__ rhs, const T *x,
+                              T *__restrict__ part, const CGScalars *sc)
 {
     if (sc->done) return;
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     int r = rbeg + t / LPR;
     int lane = t % LPR;
-    double s = 0.0;
+    T s = T(0);
     if (r < rend) {
         int a = FWD ? __ldg(&row_ptr[r]) : __ldg(&outpos[r]);
         int b = FWD ? __ldg(&inpos[r]) : __ldg(&row_ptr[r + 1]);
@@ -514,25 +515,25 @@ __global__ void k_cell_desc(int nact, const int *__restrict__ acells, const int 
 
 // Lane-per-row solve of one cell from a staged entry block (lo/up runs in
 // walk order, local column index in `ks`).  R = row slots per lane.
-template <bool FWD, int R>
-__device__ __forceinline__ void cell_solve(int r0, int m, const int *off, const int *len, double *acc,
-                                           const double *dv, const double *vals, const unsigned char *ks,
-                                           double *__restrict__ x)
+template <bool FWD, int R, class T>
+__device__ __forceinline__ void cell_solve(int r0, int m, const int *off, const int *len, T *acc,
+                                           const T *dv, const T *vals, const unsigned char *ks,
+                                           T *__restrict__ x)
 {
     int lane = threadIdx.x & 31;
     int cur[R], ck[R];
-    double cv[R];
+    T cv[R];
 #pragma unroll
     for (int j = 0; j < R; j++) {
         cur[j] = off[j];
         int end = off[j] + len[j];
         ck[j] = (cur[j] < end) ? (int)ks[cur[j]] : -1;
-        cv[j] = (cur[j] < end) ? vals[cur[j]] : 0.0;
+        cv[j] = (cur[j] < end) ? vals[cur[j]] : T(0);
     }
     for (int sidx = 0; sidx < m; sidx++) {
         int k = FWD ? sidx : m - 1 - sidx;
         int owner = k & 31;
-        double v = 0.0;
+        T v = T(0);
         if (R == 1) {
             if (lane == owner) {
                 v = acc[0] * dv[0];
@@ -555,7 +556,7 @@ __device__ __forceinline__ void cell_solve(int r0, int m, const int *off, const 
                 ++cur[j];
                 bool more = cur[j] < off[j] + len[j];
                 ck[j] = more ? (int)ks[cur[j]] : -1;
-                cv[j] = more ? vals[cur[j]] : 0.0;
+                cv[j] = more ? vals[cur[j]] : T(0);
             }
         }
     }
@@ -563,14 +564,14 @@ __device__ __forceinline__ void cell_solve(int r0, int m, const int *off, const 
 
 // In-cell solve of one colour, a warp per cell (see the section comment).
 // part[r] = rhs[r] - cross-cell sum; writes x for the cell's rows.
-template <bool FWD>
+template <bool FWD, class T>
 __global__ void __launch_bounds__(32 * CELL_WARPS)
 k_sweep_cell(int kbeg, int kend, const int2 *__restrict__ desc, const int *__restrict__ pk_off,
-             const int *__restrict__ pk_len, const double *__restrict__ pk_val,
-             const unsigned char *__restrict__ pk_k, const double *__restrict__ dinv,
-             const double *__restrict__ part, double *__restrict__ x, const CGScalars *sc)
+             const int *__restrict__ pk_len, const T *__restrict__ pk_val,
+             const unsigned char *__restrict__ pk_k, const T *__restrict__ dinv,
+             const T *__restrict__ part, T *__restrict__ x, const CGScalars *sc)
 {
-    __shared__ double s_val[CELL_WARPS][CELL_MAXE];
+    __shared__ T s_val[CELL_WARPS][CELL_MAXE];
     __shared__ unsigned char s_k[CELL_WARPS][CELL_MAXE];
     if (sc->done) return;
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -583,7 +584,7 @@ k_sweep_cell(int kbeg, int kend, const int2 *__restrict__ desc, const int *__res
         for (int t = 0; t < m; t++) {
             int r = FWD ? r0 + t : r0 + m - 1 - t;
             int o = pk_off[r], l = pk_len[r];
-            double ps = 0.0;
+            T ps = T(0);
             for (int e = lane; e < l; e += 32) ps += pk_val[o + e] * x[r0 + pk_k[o + e]];
 #pragma unroll
             for (int q = 16; q > 0; q >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, q);
@@ -594,12 +595,12 @@ k_sweep_cell(int kbeg, int kend, const int2 *__restrict__ desc, const int *__res
     }
     constexpr int R = SWEEP_MAXM / 32;
     int off[R], len[R];
-    double acc[R], dv[R];
+    T acc[R], dv[R];
 #pragma unroll
     for (int j = 0; j < R; j++) {
         int t = lane + 32 * j;
         off[j] = len[j] = 0;
-        acc[j] = dv[j] = 0.0;
+        acc[j] = dv[j] = T(0);
         if (t < m) {
             int r = r0 + t;
             off[j] = pk_off[r];
@@ -615,7 +616,7 @@ k_sweep_cell(int kbeg, int kend, const int2 *__restrict__ desc, const int *__res
 #pragma unroll
     for (int q = 16; q > 0; q >>= 1) endo = max(endo, __shfl_xor_sync(0xffffffffu, endo, q));
     int total = endo > base ? endo - base : 0;
-    const double *vals;
+    const T *vals;
     const unsigned char *ks;
     if (total <= CELL_MAXE) {
 #pragma unroll 4
@@ -632,9 +633,9 @@ k_sweep_cell(int kbeg, int kend, const int2 *__restrict__ desc, const int *__res
         vals = pk_val;
         ks = pk_k;
     }
-    if (m <= 32) cell_solve<FWD, 1>(r0, m, off, len, acc, dv, vals, ks, x);
-    else if (m <= 64) cell_solve<FWD, 2>(r0, m, off, len, acc, dv, vals, ks, x);
-    else cell_solve<FWD, 4>(r0, m, off, len, acc, dv, vals, ks, x);
+    if (m <= 32) cell_solve<FWD, 1, T>(r0, m, off, len, acc, dv, vals, ks, x);
+    else if (m <= 64) cell_solve<FWD, 2, T>(r0, m, off, len, acc, dv, vals, ks, x);
+    else cell_solve<FWD, 4, T>(r0, m, off, len, acc, dv, vals, ks, x);
 }
 
 // ---- CG vector kernels ------------------------------------------------------
@@ -654,9 +655,9 @@ __device__ __forceinline__ double final_sum(const double *partials, unsigned n, 
 // Ap = A p and the p.Ap partial; the last block forms alpha.  The kernel
 // also performs the loop-head test of the reference (sqrt(r.r) < tol, and
 // the iteration cap) before any work.
-template <int LPR>
+template <int LPR, class T>
 __global__ void k_cg_spmv(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ col,
-                          const double *__restrict__ A, const double *__restrict__ p, double *__restrict__ Ap,
+                          const T *__restrict__ A, const T *__restrict__ p, T *__restrict__ Ap,
                           double *partials, unsigned *ticket, CGScalars *sc)
 {
     __shared__ double sh[CG_BLOCK / 32];
@@ -670,7 +671,7 @@ __global__ void k_cg_spmv(int n_eq, const int *__restrict__ row_ptr, const int *
     double acc = 0.0;
     for (int rb = blockIdx.x * rows_per_block; rb < n_eq; rb += gridDim.x * rows_per_block) {
         int r = rb + threadIdx.x / LPR;
-        double s = 0.0;
+        T s = T(0);
         if (r < n_eq) {
             int q1 = __ldg(&row_ptr[r + 1]);
 #pragma unroll 4
@@ -680,7 +681,7 @@ __global__ void k_cg_spmv(int n_eq, const int *__restrict__ row_ptr, const int *
         for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LPR);
         if (lane == 0 && r < n_eq) {
             Ap[r] = s;
-            acc += p[r] * s;
+            acc += (double)p[r] * (double)s;
         }
     }
     double t = block_sum<CG_BLOCK>(acc, sh);
@@ -696,18 +697,19 @@ __global__ void k_cg_spmv(int n_eq, const int *__restrict__ row_ptr, const int *
 }
 
 // x += alpha p, r -= alpha Ap, and r.r.
-__global__ void k_cg_axpy(int n_eq, double *__restrict__ x, double *__restrict__ r, const double *__restrict__ p,
-                          const double *__restrict__ Ap, double *partials, unsigned *ticket, CGScalars *sc)
+template <class T>
+__global__ void k_cg_axpy(int n_eq, T *__restrict__ x, T *__restrict__ r, const T *__restrict__ p,
+                          const T *__restrict__ Ap, double *partials, unsigned *ticket, CGScalars *sc)
 {
     __shared__ double sh[CG_BLOCK / 32];
     if (sc->done) return;
-    double alpha = sc->alpha;
+    T alpha = (T)sc->alpha;
     double acc = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_eq; i += gridDim.x * blockDim.x) {
         x[i] += alpha * p[i];
-        double ri = r[i] - alpha * Ap[i];
+        T ri = r[i] - alpha * Ap[i];
         r[i] = ri;
-        acc += ri * ri;
+        acc += (double)ri * (double)ri;
     }
     double t = block_sum<CG_BLOCK>(acc, sh);
     if (threadIdx.x == 0) partials[blockIdx.x] = t;
@@ -718,14 +720,15 @@ __global__ void k_cg_axpy(int n_eq, double *__restrict__ x, double *__restrict__
 }
 
 // rz_new = r.z, the breakdown test on the previous rz, beta.
-__global__ void k_cg_rz(int n_eq, const double *__restrict__ r, const double *__restrict__ z,
+template <class T>
+__global__ void k_cg_rz(int n_eq, const T *__restrict__ r, const T *__restrict__ z,
                         double *partials, unsigned *ticket, CGScalars *sc)
 {
     __shared__ double sh[CG_BLOCK / 32];
     if (sc->done) return;
     double acc = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_eq; i += gridDim.x * blockDim.x)
-        acc += r[i] * z[i];
+        acc += (double)r[i] * (double)z[i];
     double t = block_sum<CG_BLOCK>(acc, sh);
     if (threadIdx.x == 0) partials[blockIdx.x] = t;
     if (last_block(ticket, gridDim.x)) {
@@ -738,35 +741,38 @@ __global__ void k_cg_rz(int n_eq, const double *__restrict__ r, const double *__
     }
 }
 
-__global__ void k_cg_update_p(int n_eq, double *__restrict__ p, const double *__restrict__ z, CGScalars *sc)
+template <class T>
+__global__ void k_cg_update_p(int n_eq, T *__restrict__ p, const T *__restrict__ z, CGScalars *sc)
 {
     if (sc->done) return;
-    double beta = sc->beta;
+    T beta = (T)sc->beta;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_eq; i += gridDim.x * blockDim.x)
         p[i] = z[i] + beta * p[i];
     if (blockIdx.x == 0 && threadIdx.x == 0) sc->iter += 1;
 }
 
 // x = 0, r = b.
-__global__ void k_cg_init(int n_eq, double *__restrict__ x, double *__restrict__ r, const double *__restrict__ b)
+template <class T>
+__global__ void k_cg_init(int n_eq, T *__restrict__ x, T *__restrict__ r, const T *__restrict__ b)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_eq; i += gridDim.x * blockDim.x) {
-        x[i] = 0.0;
+        x[i] = T(0);
         r[i] = b[i];
     }
 }
 
 // p = z, rz = r.z, rr = r.r.
-__global__ void k_cg_init2(int n_eq, const double *__restrict__ r, const double *__restrict__ z,
-                           double *__restrict__ p, double *partials, unsigned *ticket, CGScalars *sc)
+template <class T>
+__global__ void k_cg_init2(int n_eq, const T *__restrict__ r, const T *__restrict__ z,
+                           T *__restrict__ p, double *partials, unsigned *ticket, CGScalars *sc)
 {
     __shared__ double sh[CG_BLOCK / 32];
     double a = 0.0, b2 = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_eq; i += gridDim.x * blockDim.x) {
-        double ri = r[i], zi = z[i];
+        T ri = r[i], zi = z[i];
         p[i] = zi;
-        a += ri * zi;
-        b2 += ri * ri;
+        a += (double)ri * (double)zi;
+        b2 += (double)ri * (double)ri;
     }
     double ta = block_sum<CG_BLOCK>(a, sh);
     double tb = block_sum<CG_BLOCK>(b2, sh);
@@ -784,6 +790,78 @@ __global__ void k_cg_init2(int n_eq, const double *__restrict__ r, const double 
             sc->done = 0;
             sc->breakdown = 0;
         }
+    }
+}
+
+// ---- mixed precision: conversions and the FP64 refinement --------------------
+
+template <class S, class T>
+__global__ void k_convert(size_t n, const S *__restrict__ in, T *__restrict__ out)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = (T)in[i];
+}
+
+// x64 = 0, r64 = b, r32 = (float) b, ||b||^2 into sc->rr_outer.
+__global__ void k_refine_init(int n_eq, double *__restrict__ x, double *__restrict__ r, float *__restrict__ r32,
+                              const double *__restrict__ b, double *partials, unsigned *ticket, CGScalars *sc)
+{
+    __shared__ double sh[CG_BLOCK / 32];
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_eq; i += gridDim.x * blockDim.x) {
+        double bi = b[i];
+        x[i] = 0.0;
+        r[i] = bi;
+        r32[i] = (float)bi;
+        acc += bi * bi;
+    }
+    double t = block_sum<CG_BLOCK>(acc, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = t;
+    if (last_block(ticket, gridDim.x)) {
+        double tot = final_sum(partials, gridDim.x, 1, 0, sh);
+        if (threadIdx.x == 0) sc->rr_outer = tot;
+    }
+}
+
+// x64 += (double) d32; then the FP64 residual r = b - A x with the FP64
+// matrix, its FP32 copy and ||r||^2 (8 lanes per row).
+__global__ void k_refine_update(int n_eq, double *__restrict__ x, const float *__restrict__ d)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_eq; i += gridDim.x * blockDim.x)
+        x[i] += (double)d[i];
+}
+
+__global__ void k_refine_residual(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ col,
+                                  const double *__restrict__ A, const double *__restrict__ x,
+                                  const double *__restrict__ b, double *__restrict__ r, float *__restrict__ r32,
+                                  double *partials, unsigned *ticket, CGScalars *sc)
+{
+    constexpr int LPR = 8;
+    __shared__ double sh[CG_BLOCK / 32];
+    int lane = threadIdx.x % LPR;
+    int rows_per_block = CG_BLOCK / LPR;
+    double acc = 0.0;
+    for (int rb = blockIdx.x * rows_per_block; rb < n_eq; rb += gridDim.x * rows_per_block) {
+        int i = rb + threadIdx.x / LPR;
+        double s = 0.0;
+        if (i < n_eq) {
+            int q1 = __ldg(&row_ptr[i + 1]);
+            for (int q = __ldg(&row_ptr[i]) + lane; q < q1; q += LPR) s += __ldg(&A[q]) * x[__ldg(&col[q])];
+        }
+#pragma unroll
+        for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LPR);
+        if (lane == 0 && i < n_eq) {
+            double ri = b[i] - s;
+            r[i] = ri;
+            r32[i] = (float)ri;
+            acc += ri * ri;
+        }
+    }
+    double t = block_sum<CG_BLOCK>(acc, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = t;
+    if (last_block(ticket, gridDim.x)) {
+        double tot = final_sum(partials, gridDim.x, 1, 0, sh);
+        if (threadIdx.x == 0) sc->rr_outer = tot;
     }
 }
 

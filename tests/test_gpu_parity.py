@@ -303,3 +303,28 @@ def test_golden_trajectory_gpu():
     assert _rel(mine[fluid, :3], gold[fluid, :3]) < 1e-8
     assert _rel(mine[fluid, 3:6], gold[fluid, 3:6]) < 1e-6
     assert _rel(mine[:, 6], gold[:, 6]) < 1e-6
+
+
+@pytest.mark.parametrize("steps", [1, 20])
+def test_mixed_precision_against_fp64(steps):
+    """The mixed form (FP32 inner ICCG + FP64 refinement) stays within the
+    1e-4 pressure relative-L2 target of the FP64 path, from the same state."""
+    _cuda()
+    from mps_b200 import _lib
+    from mps_b200.session import start
+    wl = W.dambreak("c1", l0=0.02, seed=8)
+    cfg = wl.config()
+    h64 = T.HostParticles(3, wl.pos, wl.vel, wl.types)
+    h32 = h64.copy()
+    a = start(cfg, 3, h64)
+    b = start(cfg, 3, h32, precision=_lib.PREC_MIXED)
+    a.step(steps)
+    b.step(steps)
+    ga, gb = a.download(), b.download()
+    mb = b.metrics()
+    a.close()
+    b.close()
+    assert np.array_equal(ga["type"], gb["type"])
+    assert _rel(gb["pressure"], ga["pressure"]) < 1e-4
+    assert _rel(gb["pos"], ga["pos"]) < 1e-6
+    assert mb["ppe_outer"] >= 1 and mb["converged"] == 1
