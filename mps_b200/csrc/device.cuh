@@ -9,6 +9,7 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <cstdlib>
 
 namespace mps {
 
@@ -27,6 +28,49 @@ inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
     ++launch_counter();
 }
 
+// Programmatic dependent launch (sm_90+): the kernel may be scheduled while
+// its predecessor in the stream is still running.  Kernels launched this way
+// call pdl_trigger() first, load only data that no earlier kernel of the
+// chain writes, then call pdl_wait() on every path -- after it the
+// predecessor grid has completed and its writes are visible -- before they
+// read anything a predecessor produced or return.  MPS_PDL=0 in the
+// environment launches them as ordinary kernels (same results, bit for bit).
+inline bool pdl_enabled()
+{
+    static const bool on = [] {
+        const char *e = std::getenv("MPS_PDL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+template <class... KArgs, class... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                       Args... args)
+{
+    if (!pdl_enabled()) {
+        launch(kernel, grid, block, smem, st, args...);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+    ++launch_counter();
+}
+
+// griddepcontrol (PTX ISA 7.8): both are no-ops in a kernel launched
+// without the programmatic attribute.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 enum : int { FLUID = 0, WALL = 1, GHOST = 2, DUMMY = 3 };
 
 // Device error bits (Engine::err_), turned into MPS_ERR_* codes on the host.
@@ -36,6 +80,8 @@ enum : unsigned {
     ERR_LIST_MISMATCH     = 4u,   // caller list differs from the cell structure
     ERR_COLORING          = 8u,   // matrix couples two same-coloured cells
     ERR_CELL_OVERFULL     = 16u,  // more than 255 unknowns in one cell
+    ERR_COPY_TIMEOUT      = 32u,  // a bulk copy into shared memory did not complete in time
+    ERR_WINDOW_OVERFLOW   = 64u,  // a window of block inverses exceeded its shared-memory stage
 };
 
 // Constants of one session, evaluated on the host with the reference's

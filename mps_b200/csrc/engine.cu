@@ -215,18 +215,27 @@ private:
     DevArray<double> pk_val_lo_, pk_val_up_, dinv_;
     DevArray<unsigned char> pk_k_lo_, pk_k_up_;
     DevArray<int2> adesc_;
+    DevArray<int> inv_len_, inv_off_;        // in-cell block inverses: entries, offsets per active cell
+    DevArray<double> inv_cm_, inv_rm_;       // column-major (forward) and row-major (backward) copies
+    DevArray<int> colinv_, wfirst_;          // inverse offsets at colour boundaries; first cell per window
+    std::vector<int> nwin_, win_off_;        // windows per colour, their table offsets
 
 
     // ---- PPE
     DevArray<int> ucount_, ucol_, rs_, cell_row0_, row_of_, part_of_row_, rcount_, row_ptr_, diagpos_, col_;
     DevArray<double> A_, F_, b_, x_, r_, z_, p_, Ap_, y_, part_, partials_;
-    DevArray<float> A32_, F32_, pkv32_lo_, pkv32_up_, dinv32_, r32_, z32_, p32_, Ap32_, y32_, part32_, d32_;
+    DevArray<float> A32_, F32_, pkv32_lo_, pkv32_up_, inv32_cm_, inv32_rm_, dinv32_;
+    DevArray<float> r32_, z32_, p32_, Ap32_, y32_, part32_, d32_;
     DevArray<CGScalars> sc_;
     DevArray<unsigned> ticket_, err_;
     int n_eq_ = 0;
     long long nnz_ = 0;
+    int ninv_ = 0;            // entries of the in-cell block inverses
     int spmv_lpr_ = 8;   // lanes per row of the CG SpMV (MPS_SPMV_LPR: 8, 16 or 32)
     int cross_lpr_ = 8;  // lanes per row of the sweeps' cross-cell products (MPS_CROSS_LPR: 4, 8, 16)
+    // CG-loop kernels launched as programmatic dependents (MPS_PDL_MASK): 1 the
+    // cross-cell sweep kernel, 2 the in-cell sweep kernel, 4 SpMV and vector kernels
+    int pdl_mask_ = 4;
     bool ppe_valid_ = false;
 
     // ---- misc
@@ -260,7 +269,7 @@ private:
     void ppe(bool clamp);
     template <class T>
     struct PcgBufs {
-        const T *A, *F, *pkv_lo, *pkv_up, *dinv;
+        const T *A, *F, *pkv_lo, *pkv_up, *dinv, *inv_cm, *inv_rm;
         T *x, *r, *z, *p, *Ap, *y, *part;
         const T *b;
     };
@@ -295,6 +304,7 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
         int v = std::atoi(e);
         if (v == 8 || v == 16 || v == 32) spmv_lpr_ = v;
     }
+    if (const char *e = std::getenv("MPS_PDL_MASK")) pdl_mask_ = std::atoi(e) & 7;
     if (const char *e = std::getenv("MPS_CROSS_LPR")) {
         int v = std::atoi(e);
         if (v == 4 || v == 8 || v == 16) cross_lpr_ = v;
@@ -305,6 +315,11 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
     for (auto &e : pev_) MPS_CUDA(cudaEventCreate(&e));
     MPS_CUDA(cudaMallocHost((void **)&sc_host_, sizeof(CGScalars)));
     MPS_CUDA(cudaMallocHost((void **)&int_host_, 64 * sizeof(int)));
+    // the staged in-cell sweeps take more than the default 48 KB of dynamic shared memory
+    MPS_CUDA(cudaFuncSetAttribute(k_sweep_cell<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(double) * CELL_STAGE)));
+    MPS_CUDA(cudaFuncSetAttribute(k_sweep_cell<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(double) * CELL_STAGE)));
     alloc_state();
     build_grid();
     compute_consts();
@@ -542,6 +557,8 @@ void Engine<D>::check_err()
         if (e & ERR_LIST_MISMATCH) throw CudaError("neighbour list does not match the cell structure", MPS_ERR_UNSUPPORTED);
         if (e & ERR_COLORING) throw CudaError("PPE row count mismatch", MPS_ERR_INVALID);
         if (e & ERR_CELL_OVERFULL) throw CudaError("more than 255 PPE unknowns in one cell", MPS_ERR_UNSUPPORTED);
+        if (e & ERR_COPY_TIMEOUT) throw CudaError("a bulk copy into shared memory timed out", MPS_ERR_CUDA);
+        if (e & ERR_WINDOW_OVERFLOW) throw CudaError("in-cell inverse window exceeds its stage", MPS_ERR_INVALID);
         throw CudaError("device error", MPS_ERR_INVALID);
     }
 }
@@ -961,14 +978,48 @@ void Engine<D>::ppe(bool clamp)
         if (nact)
             launch(k_cell_desc, nblk(nact, TPB), TPB, 0, st_, nact, (const int *)acells_.p,
                    (const int *)cell_row0_.p, (const int *)ucount_.p, adesc_.p);
+        // inverses of the in-cell diagonal blocks of the factor, and the
+        // windows of each colour's range for the staged in-cell sweeps
+        inv_len_.reserve((size_t)nact + 1);
+        inv_off_.reserve((size_t)nact + 1);
+        if (nact) launch(k_inv_sizes, nblk(nact, TPB), TPB, 0, st_, nact, (const int2 *)adesc_.p, inv_len_.p);
+        scan_exclusive<int>(inv_len_.p, inv_off_.p, nact, scanws_.p, st_);
+        ColourIdx at{};
+        for (int c = 0; c <= ncol; c++) at.k[c] = act_off_[c];
+        colinv_.reserve(16);
+        launch(k_gather_colour_offsets, 1, 32, 0, st_, at, ncol + 1, (const int *)inv_off_.p, colinv_.p);
+        MPS_CUDA(cudaMemcpyAsync(int_host_, colinv_.p, sizeof(int) * (ncol + 1), cudaMemcpyDeviceToHost, st_));
+        MPS_CUDA(cudaStreamSynchronize(st_));
+        int ninv = int_host_[ncol];
+        if (ninv < 0) throw CudaError("in-cell inverses too large for 32-bit offsets", MPS_ERR_UNSUPPORTED);
+        win_off_.assign(ncol + 1, 0);
+        nwin_.assign(ncol, 0);
+        for (int c = 0; c < ncol; c++) {
+            int span = int_host_[c + 1] - int_host_[c];
+            nwin_[c] = act_off_[c + 1] > act_off_[c] ? std::max(1, (span + CELL_WIN - 1) / CELL_WIN) : 0;
+            win_off_[c + 1] = win_off_[c] + nwin_[c] + 1;
+        }
+        inv_cm_.reserve((size_t)ninv + 1);
+        inv_rm_.reserve((size_t)ninv + 1);
+        wfirst_.reserve((size_t)win_off_[ncol] + 1);
+        ninv_ = ninv;
+        if (nact)
+            launch(k_cell_inverse, nblk(nact, 4), 128, 0, st_, nact, (const int2 *)adesc_.p,
+                   (const int *)inv_off_.p, (const int *)pk_off_lo_.p, (const int *)pk_len_lo_.p,
+                   (const double *)pk_val_lo_.p, (const unsigned char *)pk_k_lo_.p, (const double *)dinv_.p,
+                   inv_cm_.p, inv_rm_.p);
+        for (int c = 0; c < ncol; c++)
+            if (nwin_[c])
+                launch(k_inv_windows, nblk(nwin_[c] + 1, TPB), TPB, 0, st_, act_off_[c], act_off_[c + 1],
+                       (const int *)inv_off_.p, nwin_[c], wfirst_.p + win_off_[c]);
     }
     MPS_CUDA(cudaEventRecord(ev_[3], st_));
 
     if (prm_.precision == MPS_PREC_MIXED) {
         mixed_solve(n_eq, nnz, icc);
     } else {
-        PcgBufs<double> v{A_.p, F_.p, pk_val_lo_.p, pk_val_up_.p, dinv_.p, x_.p, r_.p, z_.p, p_.p, Ap_.p, y_.p,
-                          part_.p, b_.p};
+        PcgBufs<double> v{A_.p,   F_.p,  pk_val_lo_.p, pk_val_up_.p, dinv_.p, inv_cm_.p, inv_rm_.p, x_.p,
+                          r_.p,   z_.p,  p_.p,         Ap_.p,        y_.p,    part_.p,   b_.p};
         pcg_solve<double>(v, prm_.cg_tolerance, prm_.cg_max_iter, icc, n_eq, nnz);
         met.ppe_iterations = sc_host_->iter;
         met.ppe_outer = 1;
@@ -998,8 +1049,14 @@ void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, 
     MPS_CUDA(cudaMemcpyAsync(sc_.p, &init, sizeof(CGScalars), cudaMemcpyHostToDevice, st_));
     launch(k_cg_init<T>, RB, CG_BLOCK, 0, st_, n_eq, v.x, v.r, v.b);
     T *z = icc ? v.z : v.r;
+    // CG-loop launch: as a programmatic dependent when its group's bit is in pdl_mask_
+    auto lk = [&](int bit, auto kern, dim3 g, dim3 b, size_t sm, auto... args) {
+        if (pdl_mask_ & bit) launch_pdl(kern, g, b, sm, st_, args...);
+        else launch(kern, g, b, sm, st_, args...);
+    };
     // IC(0) sweeps per colour: the cross-cell products of all the colour's
-    // rows, then the in-cell solve a warp per cell from staged packed runs.
+    // rows, then the in-cell product a warp per cell from the staged block
+    // inverses.
     auto sweep = [&](bool fwdir) {
         const T *rhs = fwdir ? v.r : v.y;
         T *out = fwdir ? v.y : v.z;
@@ -1012,25 +1069,28 @@ void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, 
             int rb = row_off_[c], re = row_off_[c + 1];
             if (ke <= kb) continue;
             auto crossk = fwdir ? k_sweep_cross<true, 8, T> : k_sweep_cross<false, 8, T>;
-            launch(crossk, nblk((long long)(re - rb) * 8, 256), 256, 0, st_, rb, re, (const int *)row_ptr_.p,
-                   (const int *)inpos_.p, (const int *)outpos_.p, (const int *)col_.p, v.F, rhs, (const T *)out,
-                   v.part, (const CGScalars *)sc_.p);
+            if (cross_lpr_ == 4) crossk = fwdir ? k_sweep_cross<true, 4, T> : k_sweep_cross<false, 4, T>;
+            if (cross_lpr_ == 16) crossk = fwdir ? k_sweep_cross<true, 16, T> : k_sweep_cross<false, 16, T>;
+            lk(1, crossk, nblk((long long)(re - rb) * cross_lpr_, 256), 256, 0, rb, re, (const int *)row_ptr_.p,
+               (const int *)inpos_.p, (const int *)outpos_.p, (const int *)col_.p, v.F, rhs, (const T *)out, v.part,
+               (const CGScalars *)sc_.p);
             auto cellk = fwdir ? k_sweep_cell<true, T> : k_sweep_cell<false, T>;
-            launch(cellk, nblk(ke - kb, CELL_WARPS), 32 * CELL_WARPS, 0, st_, kb, ke, (const int2 *)adesc_.p, pko,
-                   pkl, pkv, pkk, v.dinv, (const T *)v.part, out, (const CGScalars *)sc_.p);
+            lk(2, cellk, nwin_[c], CELL_THREADS, sizeof(T) * CELL_STAGE, (const int *)wfirst_.p + win_off_[c],
+               (const int2 *)adesc_.p, (const int *)inv_off_.p, fwdir ? v.inv_cm : v.inv_rm, pko, pkl, pkv, pkk,
+               v.dinv, (const T *)v.part, out, (const CGScalars *)sc_.p, err_.p);
         }
     };
     auto spmv = [&]() {
         const int *rp = row_ptr_.p, *ci = col_.p;
         if (spmv_lpr_ == 16)
-            launch(k_cg_spmv<16, T>, RB, CG_BLOCK, 0, st_, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
-                   ticket_.p, sc_.p);
+            lk(4, k_cg_spmv<16, T>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
+               ticket_.p, sc_.p);
         else if (spmv_lpr_ == 32)
-            launch(k_cg_spmv<32, T>, RB, CG_BLOCK, 0, st_, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
-                   ticket_.p, sc_.p);
+            lk(4, k_cg_spmv<32, T>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
+               ticket_.p, sc_.p);
         else
-            launch(k_cg_spmv<8, T>, RB, CG_BLOCK, 0, st_, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
-                   ticket_.p, sc_.p);
+            lk(4, k_cg_spmv<8, T>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
+               ticket_.p, sc_.p);
     };
     if (icc) { sweep(true); sweep(false); }
     launch(k_cg_init2<T>, RB, CG_BLOCK, 0, st_, n_eq, (const T *)v.r, (const T *)z, v.p, partials_.p, ticket_.p,
@@ -1043,16 +1103,15 @@ void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, 
             if (prof) MPS_CUDA(cudaEventRecord(e[0], st_));
             spmv();
             if (prof) MPS_CUDA(cudaEventRecord(e[1], st_));
-            launch(k_cg_axpy<T>, RB, CG_BLOCK, 0, st_, n_eq, v.x, v.r, (const T *)v.p, (const T *)v.Ap, partials_.p,
-                   ticket_.p, sc_.p);
+            lk(4, k_cg_axpy<T>, RB, CG_BLOCK, 0, n_eq, v.x, v.r, (const T *)v.p, (const T *)v.Ap, partials_.p,
+               ticket_.p, sc_.p);
             if (prof) MPS_CUDA(cudaEventRecord(e[2], st_));
             if (icc) sweep(true);
             if (prof) MPS_CUDA(cudaEventRecord(e[3], st_));
             if (icc) sweep(false);
             if (prof) MPS_CUDA(cudaEventRecord(e[4], st_));
-            launch(k_cg_rz<T>, RB, CG_BLOCK, 0, st_, n_eq, (const T *)v.r, (const T *)z, partials_.p, ticket_.p,
-                   sc_.p);
-            launch(k_cg_update_p<T>, RB, CG_BLOCK, 0, st_, n_eq, v.p, (const T *)z, sc_.p);
+            lk(4, k_cg_rz<T>, RB, CG_BLOCK, 0, n_eq, (const T *)v.r, (const T *)z, partials_.p, ticket_.p, sc_.p);
+            lk(4, k_cg_update_p<T>, RB, CG_BLOCK, 0, n_eq, v.p, (const T *)z, sc_.p);
         }
         MPS_CUDA(cudaGetLastError());
         MPS_CUDA(cudaMemcpyAsync(sc_host_, sc_.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, st_));
@@ -1094,6 +1153,7 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
     const int RB = RED_BLOCKS;
     size_t nz = (size_t)nnz;
     for (auto *v : {&A32_, &F32_, &pkv32_lo_, &pkv32_up_}) v->reserve(nz);
+    for (auto *v : {&inv32_cm_, &inv32_rm_}) v->reserve((size_t)ninv_ + 1);
     for (auto *v : {&dinv32_, &r32_, &z32_, &p32_, &Ap32_, &y32_, &part32_, &d32_}) v->reserve((size_t)cap_);
     launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)A_.p, A32_.p);
     if (icc) {
@@ -1101,6 +1161,10 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
         launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)pk_val_lo_.p, pkv32_lo_.p);
         launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)pk_val_up_.p, pkv32_up_.p);
         launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, (size_t)n_eq, (const double *)dinv_.p, dinv32_.p);
+        launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, (size_t)ninv_, (const double *)inv_cm_.p,
+               inv32_cm_.p);
+        launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, (size_t)ninv_, (const double *)inv_rm_.p,
+               inv32_rm_.p);
     }
     CGScalars init{};
     MPS_CUDA(cudaMemcpyAsync(sc_.p, &init, sizeof(CGScalars), cudaMemcpyHostToDevice, st_));
@@ -1114,8 +1178,8 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
     double rnorm = bnorm;
     int outer = 0, inner_total = 0;
     const int inner_max = std::min(prm_.cg_max_iter, 2000);
-    PcgBufs<float> v{A32_.p, F32_.p, pkv32_lo_.p, pkv32_up_.p, dinv32_.p, d32_.p, r32_.p, z32_.p, p32_.p, Ap32_.p,
-                     y32_.p, part32_.p, r32_.p};
+    PcgBufs<float> v{A32_.p, F32_.p,  pkv32_lo_.p, pkv32_up_.p, dinv32_.p, inv32_cm_.p, inv32_rm_.p, d32_.p,
+                     r32_.p, z32_.p,  p32_.p,      Ap32_.p,     y32_.p,    part32_.p,   r32_.p};
     while (rnorm > target && outer < kMaxOuter) {
         pcg_solve<float>(v, kInnerRtol * rnorm, inner_max, icc, n_eq, nnz);
         inner_total += sc_host_->iter;

@@ -394,18 +394,19 @@ k_ic0_incell(int kbeg, int kend, const int *__restrict__ acells, const int *__re
 // cross-cell (col >= r0 + m).  `inpos[r]` is the first in-cell position and
 // `outpos[r]` the first upper cross-cell position of row r.
 //
-// A sweep over one colour runs a warp per cell in two phases:
-//   1. the cross-cell products of every row of the cell, which depend only on
-//      finished colours: 8 lanes per row, 4 rows at a time, into shared memory;
-//   2. the in-cell triangular solve: lane l owns rows l, l+32, ...; at step k
-//      the owner of row k finishes it and broadcasts the value with a
-//      shuffle, and every lane whose row has an entry in column k applies it
-//      (each lane walks its row's in-cell run with a cursor).
-// Cells with more than SWEEP_MAXM unknowns (4x the rest density; only in a
-// blow-up) take a row-by-row path with the same result.
+// A sweep over one colour runs in two kernels:
+//   1. k_sweep_cross: the cross-cell products of every row of the colour,
+//      which depend only on finished colours, LPR lanes per row, into part;
+//   2. k_sweep_cell: the in-cell triangular solve, a warp per cell, as the
+//      product with the inverse of the cell's diagonal block of the factor
+//      (formed once per step after the factorisation, k_cell_inverse): the
+//      same preconditioner as substitution, rounded differently, with no
+//      serial chain through the cell's rows.
+// Cells with more than SWEEP_MAXM unknowns (over twice the most a cell of
+// side re holds at rest spacing; only in a blow-up) are solved row by row by
+// substitution from the packed in-cell runs.
 
-constexpr int SWEEP_MAXM = 128;
-constexpr int SWEEP_WARPS = 4;   // warps per block
+constexpr int SWEEP_MAXM = 64;
 
 // Row positions of the in-cell runs; one thread per row.
 __global__ void k_row_splits(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ diagpos,
@@ -431,34 +432,50 @@ __global__ void k_row_splits(int n_eq, const int *__restrict__ row_ptr, const in
 //
 // k_sweep_cross: every row of a colour (rows [rbeg, rend) are contiguous)
 // sums its cross-cell run against the finished colours, LPR lanes per row,
-// into part[r] = rhs[r] - sum.  k_sweep_cell: a warp per cell stages the
-// cell's in-cell runs (local column index and value) and the diagonal
-// inverses in shared memory, then runs the lane-per-row solve from there.
+// into part[r] = rhs[r] - sum.
+//
+// Both sweep kernels are launched as programmatic dependents (launch_pdl):
+// what they load before pdl_wait() -- row bounds, factor values and columns,
+// block inverses, cell descriptors -- is written once per step, before the
+// CG loop; x, part and the CG scalars are read only after it.
 
 template <bool FWD, int LPR, class T>
-__global__ void k_sweep_cross(int rbeg, int rend, const int *__restrict__ row_ptr, const int *__restrict__ inpos,
-                              const int *__restrict__ outpos, const int *__restrict__ col,
-                              const T *__restrict__ F, const T *__restrict__ rhs, const T *x,
-                              T *__restrict__ part, const CGScalars *sc)
+__global__ void __launch_bounds__(256)
+k_sweep_cross(int rbeg, int rend, const int *__restrict__ row_ptr, const int *__restrict__ inpos,
+              const int *__restrict__ outpos, const int *__restrict__ col, const T *__restrict__ F,
+              const T *rhs, const T *x, T *part, const CGScalars *sc)
 {
-    if (sc->done) return;
+    constexpr int PF = 4;   // entries per lane loaded before the wait
+    pdl_trigger();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     int r = rbeg + t / LPR;
     int lane = t % LPR;
-    T s = T(0);
+    int a = 0, b = 0;
     if (r < rend) {
-        int a = FWD ? __ldg(&row_ptr[r]) : __ldg(&outpos[r]);
-        int b = FWD ? __ldg(&inpos[r]) : __ldg(&row_ptr[r + 1]);
-#pragma unroll 4
-        for (int q = a + lane; q < b; q += LPR) s += __ldg(&F[q]) * x[__ldg(&col[q])];
+        a = FWD ? __ldg(&row_ptr[r]) : __ldg(&outpos[r]);
+        b = FWD ? __ldg(&inpos[r]) : __ldg(&row_ptr[r + 1]);
     }
+    T f[PF];
+    int c[PF];
+#pragma unroll
+    for (int u = 0; u < PF; u++) {
+        int q = a + lane + u * LPR;
+        bool ok = q < b;
+        f[u] = ok ? __ldg(&F[q]) : T(0);
+        c[u] = ok ? __ldg(&col[q]) : -1;
+    }
+    pdl_wait();
+    if (sc->done) return;
+    T s = T(0);
+#pragma unroll
+    for (int u = 0; u < PF; u++)
+        if (c[u] >= 0) s += f[u] * x[c[u]];
+#pragma unroll 4
+    for (int q = a + lane + PF * LPR; q < b; q += LPR) s += __ldg(&F[q]) * x[__ldg(&col[q])];
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LPR);
     if (lane == 0 && r < rend) part[r] = rhs[r] - s;
 }
-
-constexpr int CELL_MAXE = 1536;  // staged in-cell entries per warp (larger cells read the packed runs directly)
-constexpr int CELL_WARPS = 2;    // warps per block of k_sweep_cell
 
 // Packed in-cell factor, built once per step after the factorisation.  For
 // every row r, lo: its in-cell lower entries in ascending column order
@@ -513,132 +530,267 @@ __global__ void k_cell_desc(int nact, const int *__restrict__ acells, const int 
     desc[k] = make_int2(cell_row0[c], ucount[c]);
 }
 
-// Lane-per-row solve of one cell from a staged entry block (lo/up runs in
-// walk order, local column index in `ks`).  R = row slots per lane.
-template <bool FWD, int R, class T>
-__device__ __forceinline__ void cell_solve(int r0, int m, const int *off, const int *len, T *acc,
-                                           const T *dv, const T *vals, const unsigned char *ks,
-                                           T *__restrict__ x)
+// ---- in-cell block inverses ---------------------------------------------------
+//
+// The in-cell diagonal block L_cc of the factor is inverted once per step, so
+// that the in-cell part of a sweep is a dense triangular product, a warp per
+// cell with no serial chain.  Each cell of at most SWEEP_MAXM unknowns owns
+// m(m+1)/2 entries (padded to a multiple of 4) at inv_off[k] in two layouts:
+//   column-major (forward sweep):  (L^-1)_{ij}, i >= j, at colofs(j) + i - j,
+//   row-major    (backward sweep): (L^-1)_{ji}, i <= j, at j(j+1)/2 + i,
+// so that at step j the warp's lanes read consecutive addresses.
+
+__host__ __device__ __forceinline__ int tri_colofs(int j, int m) { return j * m - (j * (j - 1)) / 2; }
+
+// Entries of every active cell's inverse, padded to a multiple of 4 so that
+// every block starts 16-byte aligned in both the FP64 and FP32 copies (0 for
+// cells above SWEEP_MAXM).
+__global__ void k_inv_sizes(int nact, const int2 *__restrict__ desc, int *__restrict__ len)
+{
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nact) return;
+    int m = desc[k].y;
+    len[k] = m <= SWEEP_MAXM ? ((m * (m + 1) / 2) + 3) & ~3 : 0;
+}
+
+// Column c of L_cc^-1 by forward substitution over the packed lower runs,
+// lane per column (columns lane and lane + 32), rows in order:
+//   X_ic = (delta_ic - sum_{c <= k < i} L_ik X_kc) / L_ii.
+// The rows' runs are read by all lanes at once; X is kept in the
+// column-major output and mirrored into the row-major one.
+__global__ void __launch_bounds__(128)
+k_cell_inverse(int nact, const int2 *__restrict__ desc, const int *__restrict__ inv_off,
+               const int *__restrict__ pk_off, const int *__restrict__ pk_len, const double *__restrict__ pk_val,
+               const unsigned char *__restrict__ pk_k, const double *__restrict__ dinv, double *inv_cm,
+               double *__restrict__ inv_rm)
 {
     int lane = threadIdx.x & 31;
-    int cur[R], ck[R];
-    T cv[R];
+    int kk = blockIdx.x * 4 + (threadIdx.x >> 5);
+    if (kk >= nact) return;
+    int2 dd = desc[kk];
+    int r0 = dd.x, m = dd.y;
+    if (m > SWEEP_MAXM) return;
+    double *cm = inv_cm + inv_off[kk];
+    double *rm = inv_rm + inv_off[kk];
+    for (int i = 0; i < m; i++) {
+        int r = r0 + i;
+        int ro = pk_off[r], rl = pk_len[r];
+        double di = dinv[r];
 #pragma unroll
-    for (int j = 0; j < R; j++) {
-        cur[j] = off[j];
-        int end = off[j] + len[j];
-        ck[j] = (cur[j] < end) ? (int)ks[cur[j]] : -1;
-        cv[j] = (cur[j] < end) ? vals[cur[j]] : T(0);
-    }
-    for (int sidx = 0; sidx < m; sidx++) {
-        int k = FWD ? sidx : m - 1 - sidx;
-        int owner = k & 31;
-        T v = T(0);
-        if (R == 1) {
-            if (lane == owner) {
-                v = acc[0] * dv[0];
-                x[r0 + k] = v;
+        for (int j = 0; j < SWEEP_MAXM / 32; j++) {
+            int c = lane + 32 * j;
+            if (c > i) continue;
+            const double *xc = cm + tri_colofs(c, m) - c;   // X_kc at xc[k]
+            double s = (c == i) ? 1.0 : 0.0;
+            for (int e = 0; e < rl; e++) {
+                int k = pk_k[ro + e];
+                if (k >= c) s -= pk_val[ro + e] * xc[k];
             }
-        } else {
-            int slot = k >> 5;
-#pragma unroll
-            for (int j = 0; j < R; j++)
-                if (j == slot && lane == owner) {
-                    v = acc[j] * dv[j];
-                    x[r0 + k] = v;
-                }
-        }
-        v = __shfl_sync(0xffffffffu, v, owner);
-#pragma unroll
-        for (int j = 0; j < R; j++) {
-            if (ck[j] == k) {
-                acc[j] -= cv[j] * v;
-                ++cur[j];
-                bool more = cur[j] < off[j] + len[j];
-                ck[j] = more ? (int)ks[cur[j]] : -1;
-                cv[j] = more ? vals[cur[j]] : T(0);
-            }
+            double v = s * di;
+            cm[tri_colofs(c, m) + i - c] = v;
+            rm[i * (i + 1) / 2 + c] = v;
         }
     }
 }
 
-// In-cell solve of one colour, a warp per cell (see the section comment).
-// part[r] = rhs[r] - cross-cell sum; writes x for the cell's rows.
-template <bool FWD, class T>
-__global__ void __launch_bounds__(32 * CELL_WARPS)
-k_sweep_cell(int kbeg, int kend, const int2 *__restrict__ desc, const int *__restrict__ pk_off,
-             const int *__restrict__ pk_len, const T *__restrict__ pk_val,
-             const unsigned char *__restrict__ pk_k, const T *__restrict__ dinv,
-             const T *__restrict__ part, T *__restrict__ x, const CGScalars *sc)
+// ---- bulk copies into shared memory (cp.async.bulk + mbarrier) ----------------
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
 {
-    __shared__ T s_val[CELL_WARPS][CELL_MAXE];
-    __shared__ unsigned char s_k[CELL_WARPS][CELL_MAXE];
-    if (sc->done) return;
-    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int kk = kbeg + blockIdx.x * CELL_WARPS + w;
-    if (kk >= kend) return;
-    int2 dd = desc[kk];
-    int r0 = dd.x, m = dd.y;
-    if (m > SWEEP_MAXM) {
-        // larger than the lane slots: row by row from the packed runs
-        for (int t = 0; t < m; t++) {
-            int r = FWD ? r0 + t : r0 + m - 1 - t;
-            int o = pk_off[r], l = pk_len[r];
-            T ps = T(0);
-            for (int e = lane; e < l; e += 32) ps += pk_val[o + e] * x[r0 + pk_k[o + e]];
-#pragma unroll
-            for (int q = 16; q > 0; q >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, q);
-            if (lane == 0) x[r] = (part[r] - ps) * dinv[r];
-            __syncwarp();
-        }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// One bulk copy global -> shared of `bytes` (a multiple of 16; both
+// addresses 16-byte aligned), completing on the mbarrier at `bar`.
+__device__ __forceinline__ void bulk_g2s(unsigned dst, const void *src, unsigned bytes, unsigned bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(__cvta_generic_to_global(src)), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// Bounded wait for phase `parity` of the mbarrier: false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, int limit)
+{
+    for (int i = 0; i < limit; i++) {
+        unsigned done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+constexpr int MBAR_POLLS = 1 << 20;
+
+// ---- staged in-cell sweep -----------------------------------------------------
+//
+// The cells of one colour are consecutive in the block-inverse arrays, so a
+// colour splits into windows of CELL_WIN entries: window w holds the cells
+// whose blocks start in [w CELL_WIN, (w+1) CELL_WIN) of the colour's range,
+// one contiguous run of at most CELL_STAGE entries.  A CTA per window copies
+// its run into shared memory with one bulk copy, issued before pdl_wait() so
+// that it overlaps the preceding cross-cell kernel, then its warps take the
+// window's cells in turn.
+
+constexpr int CELL_WIN = 4096;
+constexpr int CELL_MAXBLK = ((SWEEP_MAXM * (SWEEP_MAXM + 1) / 2) + 3) & ~3;
+constexpr int CELL_STAGE = CELL_WIN + CELL_MAXBLK;
+constexpr int CELL_THREADS = 512;
+
+// First cell of every window of one colour (cells [kbeg, kend)); entry nwin
+// is kend.  Lower bound of the window start among the cells' offsets.
+__global__ void k_inv_windows(int kbeg, int kend, const int *__restrict__ inv_off, int nwin, int *__restrict__ wfirst)
+{
+    int w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w > nwin) return;
+    if (w == nwin) {
+        wfirst[w] = kend;
         return;
     }
-    constexpr int R = SWEEP_MAXM / 32;
-    int off[R], len[R];
-    T acc[R], dv[R];
-#pragma unroll
-    for (int j = 0; j < R; j++) {
-        int t = lane + 32 * j;
-        off[j] = len[j] = 0;
-        acc[j] = dv[j] = T(0);
-        if (t < m) {
-            int r = r0 + t;
-            off[j] = pk_off[r];
-            len[j] = pk_len[r];
-            acc[j] = part[r];
-            dv[j] = dinv[r];
-        }
+    int target = inv_off[kbeg] + w * CELL_WIN;
+    int lo = kbeg, hi = kend;
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (inv_off[mid] < target) lo = mid + 1;
+        else hi = mid;
     }
-    int base = __shfl_sync(0xffffffffu, off[0], 0);
-    int endo = 0;
+    wfirst[w] = lo;
+}
+
+struct ColourIdx {
+    int k[9];
+};
+
+// inv_off at the colour boundaries (the colours' ranges and the total).
+__global__ void k_gather_colour_offsets(ColourIdx at, int n, const int *__restrict__ inv_off, int *__restrict__ out)
+{
+    int t = threadIdx.x;
+    if (t < n) out[t] = inv_off[at.k[t]];
+}
+
+// In-cell step of one colour: x = L_cc^-1 part (forward) or L_cc^-T part
+// (backward) for every cell of the window, a warp per cell, lane l owning
+// rows l and l + 32; part[r] = rhs[r] - the cross-cell sum.  Cells above
+// SWEEP_MAXM unknowns are solved row by row by substitution from the packed
+// runs.
+template <bool FWD, class T>
+__global__ void __launch_bounds__(CELL_THREADS, 4)
+k_sweep_cell(const int *__restrict__ wfirst, const int2 *__restrict__ desc, const int *__restrict__ inv_off,
+             const T *__restrict__ inv, const int *__restrict__ pk_off, const int *__restrict__ pk_len,
+             const T *__restrict__ pk_val, const unsigned char *__restrict__ pk_k, const T *__restrict__ dinv,
+             const T *part, T *x, const CGScalars *sc, unsigned *err)
+{
+    extern __shared__ __align__(128) unsigned char cell_stage[];
+    __shared__ __align__(8) unsigned long long bar;
+    pdl_trigger();
+    T *stage = reinterpret_cast<T *>(cell_stage);
+    int ka = __ldg(&wfirst[blockIdx.x]), kb = __ldg(&wfirst[blockIdx.x + 1]);
+    int o0 = 0, nel = 0;
+    if (ka < kb) {
+        o0 = __ldg(&inv_off[ka]);
+        nel = __ldg(&inv_off[kb]) - o0;
+    }
+    bool staged = nel > 0 && nel <= CELL_STAGE;
+    unsigned b = smem_u32(&bar);
+    if (threadIdx.x == 0 && staged) mbar_init(b, 1);
+    __syncthreads();
+    if (threadIdx.x == 0 && staged) {
+        unsigned bytes = (unsigned)nel * (unsigned)sizeof(T);
+        mbar_arrive_expect_tx(b, bytes);
+        bulk_g2s(smem_u32(stage), inv + o0, bytes, b);
+    }
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int k = ka + w;
+    int2 dd = make_int2(0, 0);
+    int ok = 0;
+    if (k < kb) {
+        dd = __ldg(&desc[k]);
+        ok = __ldg(&inv_off[k]);
+    }
+    pdl_wait();
+    if (staged && !mbar_wait(b, 0, MBAR_POLLS)) {
+        if (threadIdx.x == 0) atomicOr(err, ERR_COPY_TIMEOUT);
+        mbar_wait(b, 0, MBAR_POLLS);
+        return;
+    }
+    if (nel > CELL_STAGE && threadIdx.x == 0) atomicOr(err, ERR_WINDOW_OVERFLOW);
+    if (sc->done) return;
+    const T *src = staged ? stage : inv + o0;
+    for (; k < kb; k += CELL_THREADS / 32) {
+        int r0 = dd.x, m = dd.y;
+        const T *blk = src + (ok - o0);
+        int kn = k + CELL_THREADS / 32;
+        if (kn < kb) {
+            dd = __ldg(&desc[kn]);
+            ok = __ldg(&inv_off[kn]);
+        }
+        if (m > SWEEP_MAXM) {
+            for (int t = 0; t < m; t++) {
+                int r = FWD ? r0 + t : r0 + m - 1 - t;
+                int po = pk_off[r], l = pk_len[r];
+                T ps = T(0);
+                for (int e = lane; e < l; e += 32) ps += pk_val[po + e] * x[r0 + pk_k[po + e]];
 #pragma unroll
-    for (int j = 0; j < R; j++) endo = max(endo, len[j] > 0 ? off[j] + len[j] : 0);
-#pragma unroll
-    for (int q = 16; q > 0; q >>= 1) endo = max(endo, __shfl_xor_sync(0xffffffffu, endo, q));
-    int total = endo > base ? endo - base : 0;
-    const T *vals;
-    const unsigned char *ks;
-    if (total <= CELL_MAXE) {
+                for (int q = 16; q > 0; q >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, q);
+                if (lane == 0) x[r] = (part[r] - ps) * dinv[r];
+                __syncwarp();
+            }
+            continue;
+        }
+        int i0 = lane, i1 = lane + 32;
+        T p0 = i0 < m ? part[r0 + i0] : T(0);
+        T p1 = i1 < m ? part[r0 + i1] : T(0);
+        T a0 = T(0), a1 = T(0);
+        if (m <= 32) {
 #pragma unroll 4
-        for (int e = lane; e < total; e += 32) {
-            s_val[w][e] = pk_val[base + e];
-            s_k[w][e] = pk_k[base + e];
+            for (int j = 0; j < m; j++) {
+                T pj = __shfl_sync(0xffffffffu, p0, j);
+                if (FWD) {
+                    if (i0 >= j && i0 < m) a0 += blk[tri_colofs(j, m) + i0 - j] * pj;
+                } else {
+                    if (i0 <= j) a0 += blk[j * (j + 1) / 2 + i0] * pj;
+                }
+            }
+        } else {
+#pragma unroll 2
+            for (int j = 0; j < m; j++) {
+                T pj = __shfl_sync(0xffffffffu, j < 32 ? p0 : p1, j & 31);
+                if (FWD) {
+                    const T *cj = blk + tri_colofs(j, m) - j;
+                    if (i0 >= j) a0 += cj[i0] * pj;
+                    if (i1 >= j && i1 < m) a1 += cj[i1] * pj;
+                } else {
+                    const T *rj = blk + j * (j + 1) / 2;
+                    if (i0 <= j) a0 += rj[i0] * pj;
+                    if (i1 <= j) a1 += rj[i1] * pj;
+                }
+            }
         }
-        __syncwarp();
-#pragma unroll
-        for (int j = 0; j < R; j++) off[j] -= base;
-        vals = s_val[w];
-        ks = s_k[w];
-    } else {
-        vals = pk_val;
-        ks = pk_k;
+        if (i0 < m) x[r0 + i0] = a0;
+        if (i1 < m) x[r0 + i1] = a1;
     }
-    if (m <= 32) cell_solve<FWD, 1, T>(r0, m, off, len, acc, dv, vals, ks, x);
-    else if (m <= 64) cell_solve<FWD, 2, T>(r0, m, off, len, acc, dv, vals, ks, x);
-    else cell_solve<FWD, 4, T>(r0, m, off, len, acc, dv, vals, ks, x);
 }
 
 // ---- CG vector kernels ------------------------------------------------------
+//
+// The kernels of one CG iteration (SpMV, axpy, the sweeps, r.z, p update) are
+// launched as programmatic dependents of one another: each waits for its
+// predecessor before it touches a vector or the scalars, so only the launch
+// latency overlaps.
 
 constexpr int CG_BLOCK = 256;
 
@@ -657,10 +809,12 @@ __device__ __forceinline__ double final_sum(const double *partials, unsigned n, 
 // the iteration cap) before any work.
 template <int LPR, class T>
 __global__ void k_cg_spmv(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ col,
-                          const T *__restrict__ A, const T *__restrict__ p, T *__restrict__ Ap,
+                          const T *__restrict__ A, const T *p, T *Ap,
                           double *partials, unsigned *ticket, CGScalars *sc)
 {
     __shared__ double sh[CG_BLOCK / 32];
+    pdl_trigger();
+    pdl_wait();
     if (sc->done) return;
     if (sqrt(sc->rr) < sc->tol || sc->iter >= sc->maxit) {
         if (blockIdx.x == 0 && threadIdx.x == 0) sc->done = 1;
@@ -698,10 +852,12 @@ __global__ void k_cg_spmv(int n_eq, const int *__restrict__ row_ptr, const int *
 
 // x += alpha p, r -= alpha Ap, and r.r.
 template <class T>
-__global__ void k_cg_axpy(int n_eq, T *__restrict__ x, T *__restrict__ r, const T *__restrict__ p,
-                          const T *__restrict__ Ap, double *partials, unsigned *ticket, CGScalars *sc)
+__global__ void k_cg_axpy(int n_eq, T *x, T *r, const T *p, const T *Ap, double *partials, unsigned *ticket,
+                          CGScalars *sc)
 {
     __shared__ double sh[CG_BLOCK / 32];
+    pdl_trigger();
+    pdl_wait();
     if (sc->done) return;
     T alpha = (T)sc->alpha;
     double acc = 0.0;
@@ -721,10 +877,11 @@ __global__ void k_cg_axpy(int n_eq, T *__restrict__ x, T *__restrict__ r, const 
 
 // rz_new = r.z, the breakdown test on the previous rz, beta.
 template <class T>
-__global__ void k_cg_rz(int n_eq, const T *__restrict__ r, const T *__restrict__ z,
-                        double *partials, unsigned *ticket, CGScalars *sc)
+__global__ void k_cg_rz(int n_eq, const T *r, const T *z, double *partials, unsigned *ticket, CGScalars *sc)
 {
     __shared__ double sh[CG_BLOCK / 32];
+    pdl_trigger();
+    pdl_wait();
     if (sc->done) return;
     double acc = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_eq; i += gridDim.x * blockDim.x)
@@ -742,8 +899,10 @@ __global__ void k_cg_rz(int n_eq, const T *__restrict__ r, const T *__restrict__
 }
 
 template <class T>
-__global__ void k_cg_update_p(int n_eq, T *__restrict__ p, const T *__restrict__ z, CGScalars *sc)
+__global__ void k_cg_update_p(int n_eq, T *p, const T *z, CGScalars *sc)
 {
+    pdl_trigger();
+    pdl_wait();
     if (sc->done) return;
     T beta = (T)sc->beta;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_eq; i += gridDim.x * blockDim.x)

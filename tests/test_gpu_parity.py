@@ -328,3 +328,45 @@ def test_mixed_precision_against_fp64(steps):
     assert _rel(gb["pressure"], ga["pressure"]) < 1e-4
     assert _rel(gb["pos"], ga["pos"]) < 1e-6
     assert mb["ppe_outer"] >= 1 and mb["converged"] == 1
+
+
+_PDL_SCRIPT = r"""
+import sys
+import numpy as np
+from mps_b200 import types as T, workloads as W, _lib
+from mps_b200.session import start
+wl = W.dambreak("c1", l0=0.02, seed=9)
+h = T.HostParticles(3, wl.pos, wl.vel, wl.types)
+out = {}
+for name, prec in (("fp64", _lib.PREC_FP64), ("mixed", _lib.PREC_MIXED)):
+    hp = h.copy()
+    s = start(wl.config(), 3, hp, precision=prec)
+    s.step(3)
+    g = s.download()
+    out[name + "_p"] = g["pressure"].copy()
+    out[name + "_x"] = g["pos"].copy()
+    out[name + "_it"] = np.array([s.metrics()["total_iterations"]])
+    s.close()
+np.savez(sys.argv[1], **out)
+"""
+
+
+def test_programmatic_launch_is_bit_identical(tmp_path):
+    """The CG loop's programmatic dependent launches change no bit: three
+    steps with them (the default) and with MPS_PDL=0 give identical
+    pressures, positions and iteration counts, FP64 and mixed."""
+    _cuda()
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    res = {}
+    for flag in ("1", "0"):
+        f = tmp_path / f"pdl{flag}.npz"
+        env = dict(os.environ, MPS_PDL=flag, PYTHONPATH=root)
+        r = subprocess.run([sys.executable, "-c", _PDL_SCRIPT, str(f)], cwd=root, env=env, capture_output=True,
+                           text=True, timeout=600)
+        assert r.returncode == 0, r.stdout + r.stderr
+        res[flag] = np.load(f)
+    for k in res["1"].files:
+        assert np.array_equal(res["1"][k], res["0"][k]), k
