@@ -225,7 +225,7 @@ private:
     DevArray<int> ucount_, ucol_, rs_, cell_row0_, row_of_, part_of_row_, rcount_, row_ptr_, diagpos_, col_;
     DevArray<double> A_, F_, b_, x_, r_, z_, p_, Ap_, y_, part_, partials_;
     DevArray<float> A32_, F32_, pkv32_lo_, pkv32_up_, inv32_cm_, inv32_rm_, dinv32_;
-    DevArray<float> r32_, z32_, p32_, Ap32_, y32_, part32_, d32_;
+    DevArray<float> r32_, z32_, p32_, Ap32_, y32_, part32_, d32_, zprev32_;
     DevArray<CGScalars> sc_;
     DevArray<unsigned> ticket_, err_;
     int n_eq_ = 0;
@@ -274,10 +274,11 @@ private:
         const T *b;
     };
     template <class T>
-    void pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, int n_eq, long long nnz);
+    void pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, int n_eq, long long nnz,
+                   const T *zprev = nullptr);
     void mixed_solve(int n_eq, long long nnz, bool icc);
-    static constexpr int kMaxOuter = 20;         // refinement sweeps of the mixed form
-    static constexpr double kInnerRtol = 1.0e-5; // FP32 inner solve: residual reduction per sweep
+    static constexpr int kMaxUpdates = 200;      // reliable updates of the mixed form, at most
+    static constexpr double kDelta = 0.1;        // FP32 residual reduction between reliable updates
     int read_int(const int *dev);
     void check_err();
     void upload_list(const int *nb, const int *cnt, int max_nb);
@@ -1039,15 +1040,23 @@ void Engine<D>::ppe(bool clamp)
 // scalars in *sc_host_.
 template <int D>
 template <class T>
-void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, int n_eq, long long nnz)
+void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, int n_eq, long long nnz,
+                          const T *zprev)
 {
     int ncol = 1 << D;
     const int RB = RED_BLOCKS;
-    CGScalars init{};
-    init.tol = tol;
-    init.maxit = maxit;
-    MPS_CUDA(cudaMemcpyAsync(sc_.p, &init, sizeof(CGScalars), cudaMemcpyHostToDevice, st_));
-    launch(k_cg_init<T>, RB, CG_BLOCK, 0, st_, n_eq, v.x, v.r, v.b);
+    int iter_before = 0;
+    if (!zprev) {
+        CGScalars init{};
+        init.tol = tol;
+        init.maxit = maxit;
+        MPS_CUDA(cudaMemcpyAsync(sc_.p, &init, sizeof(CGScalars), cudaMemcpyHostToDevice, st_));
+        launch(k_cg_init<T>, RB, CG_BLOCK, 0, st_, n_eq, v.x, v.r, v.b);
+    } else {
+        // resumed after a reliable update: the scalars of the stopped loop stay
+        iter_before = sc_host_->iter;
+        MPS_CUDA(cudaMemsetAsync(&sc_.p->done, 0, sizeof(int), st_));
+    }
     T *z = icc ? v.z : v.r;
     // CG-loop launch: as a programmatic dependent when its group's bit is in pdl_mask_
     auto lk = [&](int bit, auto kern, dim3 g, dim3 b, size_t sm, auto... args) {
@@ -1093,9 +1102,12 @@ void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, 
                ticket_.p, sc_.p);
     };
     if (icc) { sweep(true); sweep(false); }
-    launch(k_cg_init2<T>, RB, CG_BLOCK, 0, st_, n_eq, (const T *)v.r, (const T *)z, v.p, partials_.p, ticket_.p,
-           sc_.p);
-    int iter_before = 0;
+    if (!zprev)
+        launch(k_cg_init2<T>, RB, CG_BLOCK, 0, st_, n_eq, (const T *)v.r, (const T *)z, v.p, partials_.p, ticket_.p,
+               sc_.p);
+    else
+        launch(k_reliable_fix<T>, RB, CG_BLOCK, 0, st_, n_eq, (const T *)v.r, (const T *)z, zprev, v.p, tol,
+               partials_.p, ticket_.p, sc_.p);
     for (;;) {
         bool prof = profiling;
         for (int it = 0; it < CG_BATCH; it++) {
@@ -1144,9 +1156,12 @@ void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, 
     }
 }
 
-// Mixed form: FP32 inner ICCG on A rounded to FP32 and the FP32-rounded
-// factor, corrected by FP64 iterative refinement, r = b - A x with the FP64
-// A and x, until ||r|| <= max(cg_tolerance, refine_tolerance * ||b||).
+// Mixed form: one ICCG in FP32 (A and the factor rounded to FP32, FP64 dot
+// products) with reliable updates.  Whenever its recursive residual has
+// fallen by kDelta since the last update, the FP32 iterate is folded into the
+// FP64 solution, the true residual r = b - A x is recomputed with the FP64
+// matrix, and the iteration resumes from it with its search direction kept.
+// Stops when ||r|| <= max(cg_tolerance, refine_tolerance * ||b||).
 template <int D>
 void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
 {
@@ -1154,7 +1169,8 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
     size_t nz = (size_t)nnz;
     for (auto *v : {&A32_, &F32_, &pkv32_lo_, &pkv32_up_}) v->reserve(nz);
     for (auto *v : {&inv32_cm_, &inv32_rm_}) v->reserve((size_t)ninv_ + 1);
-    for (auto *v : {&dinv32_, &r32_, &z32_, &p32_, &Ap32_, &y32_, &part32_, &d32_}) v->reserve((size_t)cap_);
+    for (auto *v : {&dinv32_, &r32_, &z32_, &p32_, &Ap32_, &y32_, &part32_, &d32_, &zprev32_})
+        v->reserve((size_t)cap_);
     launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)A_.p, A32_.p);
     if (icc) {
         launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)F_.p, F32_.p);
@@ -1176,27 +1192,35 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
     double rtol = prm_.refine_tolerance > 0.0 ? prm_.refine_tolerance : 1.0e-10;
     double target = std::max(prm_.cg_tolerance, rtol * bnorm);
     double rnorm = bnorm;
-    int outer = 0, inner_total = 0;
-    const int inner_max = std::min(prm_.cg_max_iter, 2000);
+    int updates = 0;
     PcgBufs<float> v{A32_.p, F32_.p,  pkv32_lo_.p, pkv32_up_.p, dinv32_.p, inv32_cm_.p, inv32_rm_.p, d32_.p,
                      r32_.p, z32_.p,  p32_.p,      Ap32_.p,     y32_.p,    part32_.p,   r32_.p};
-    while (rnorm > target && outer < kMaxOuter) {
-        pcg_solve<float>(v, kInnerRtol * rnorm, inner_max, icc, n_eq, nnz);
-        inner_total += sc_host_->iter;
-        launch(k_refine_update, RB, CG_BLOCK, 0, st_, n_eq, x_.p, (const float *)d32_.p);
-        launch(k_refine_residual, RB, CG_BLOCK, 0, st_, n_eq, (const int *)row_ptr_.p, (const int *)col_.p,
-               (const double *)A_.p, (const double *)x_.p, (const double *)b_.p, r_.p, r32_.p, partials_.p,
-               ticket_.p, sc_.p);
-        MPS_CUDA(cudaMemcpyAsync(sc_host_, sc_.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, st_));
-        MPS_CUDA(cudaStreamSynchronize(st_));
-        rnorm = std::sqrt(sc_host_->rr_outer);
-        outer++;
+    const float *zsrc = icc ? z32_.p : r32_.p;   // the preconditioned residual of the FP32 loop
+    if (rnorm > target) {
+        pcg_solve<float>(v, std::max(target, kDelta * rnorm), prm_.cg_max_iter, icc, n_eq, nnz);
+        for (;;) {
+            MPS_CUDA(cudaMemcpyAsync(zprev32_.p, zsrc, sizeof(float) * n_eq, cudaMemcpyDeviceToDevice, st_));
+            launch(k_refine_update, RB, CG_BLOCK, 0, st_, n_eq, x_.p, d32_.p);
+            launch(k_refine_residual, RB, CG_BLOCK, 0, st_, n_eq, (const int *)row_ptr_.p, (const int *)col_.p,
+                   (const double *)A_.p, (const double *)x_.p, (const double *)b_.p, r_.p, r32_.p, partials_.p,
+                   ticket_.p, sc_.p);
+            MPS_CUDA(cudaMemcpyAsync(sc_host_, sc_.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, st_));
+            MPS_CUDA(cudaStreamSynchronize(st_));
+            rnorm = std::sqrt(sc_host_->rr_outer);
+            updates++;
+            if (rnorm <= target || sc_host_->iter >= prm_.cg_max_iter || sc_host_->breakdown ||
+                updates >= kMaxUpdates)
+                break;
+            pcg_solve<float>(v, std::max(target, kDelta * rnorm), prm_.cg_max_iter, icc, n_eq, nnz,
+                             (const float *)zprev32_.p);
+        }
     }
-    met.ppe_iterations = inner_total;
-    met.ppe_outer = outer;
+    int inner = sc_host_->iter;
+    met.ppe_iterations = inner;
+    met.ppe_outer = updates;
     met.ppe_residual = rnorm;
     met.converged = rnorm <= target;
-    met.total_iterations += inner_total;
+    met.total_iterations += inner;
 }
 
 // ---- introspection --------------------------------------------------------

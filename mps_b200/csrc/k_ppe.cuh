@@ -984,10 +984,48 @@ __global__ void k_refine_init(int n_eq, double *__restrict__ x, double *__restri
 
 // x64 += (double) d32; then the FP64 residual r = b - A x with the FP64
 // matrix, its FP32 copy and ||r||^2 (8 lanes per row).
-__global__ void k_refine_update(int n_eq, double *__restrict__ x, const float *__restrict__ d)
+__global__ void k_refine_update(int n_eq, double *__restrict__ x, float *__restrict__ d)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_eq; i += gridDim.x * blockDim.x)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_eq; i += gridDim.x * blockDim.x) {
         x[i] += (double)d[i];
+        d[i] = 0.0f;
+    }
+}
+
+// Reliable update of the FP32 CG (mixed form): r now holds the FP32 copy of
+// the true FP64 residual and z its preconditioned value; the search
+// direction keeps its history, p = z + beta p_prev with the new z, i.e.
+// p += z - zprev.  New r.z and r.r; the inner loop resumes with `tol`.
+template <class T>
+__global__ void k_reliable_fix(int n_eq, const T *__restrict__ r, const T *__restrict__ z,
+                               const T *__restrict__ zprev, T *__restrict__ p, double tol, double *partials,
+                               unsigned *ticket, CGScalars *sc)
+{
+    __shared__ double sh[CG_BLOCK / 32];
+    double a = 0.0, b2 = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_eq; i += gridDim.x * blockDim.x) {
+        T ri = r[i], zi = z[i];
+        p[i] = p[i] + (zi - zprev[i]);
+        a += (double)ri * (double)zi;
+        b2 += (double)ri * (double)ri;
+    }
+    double ta = block_sum<CG_BLOCK>(a, sh);
+    double tb = block_sum<CG_BLOCK>(b2, sh);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = ta;
+        partials[2 * blockIdx.x + 1] = tb;
+    }
+    if (last_block(ticket, gridDim.x)) {
+        double sa = final_sum(partials, gridDim.x, 2, 0, sh);
+        double sb = final_sum(partials, gridDim.x, 2, 1, sh);
+        if (threadIdx.x == 0) {
+            sc->rz = sa;
+            sc->rr = sb;
+            sc->tol = tol;
+            sc->done = 0;
+            sc->breakdown = 0;
+        }
+    }
 }
 
 __global__ void k_refine_residual(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ col,
