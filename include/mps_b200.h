@@ -204,6 +204,44 @@ void *mps_get_stream(mps_session *s);
 int  mps_run_stage(mps_session *s, int stage, const int *neighbors, const int *count,
                    int max_nb, double arg);
 
+/* ---- differentiation form (adjoint of the time step) --------------------
+ *
+ * No counterpart in the reference, which has no adjoint and no restart
+ * format (its CSV output loses n0 / lambda and the sort state).
+ *
+ * Checkpoints.  mps_state_bytes gives the size of one checkpoint of the
+ * session's current state (positions, velocities, sort keys, pressures,
+ * flags, reference indices and the cell structure: all the next step
+ * reads).  mps_state_save / mps_state_load copy it to / from a caller
+ * buffer in host or device memory; loading and stepping reproduces the
+ * saved run bit for bit.  A checkpoint only loads into the session that
+ * wrote it (same capacity and grid).
+ *
+ * Adjoint.  mps_adjoint_seed sets the adjoint of a step's output state:
+ * lam_pos, lam_vel are host arrays of num*dim doubles in reference particle
+ * order (particle-major; NULL = zero); it also clears the accumulated
+ * parameter gradients.  With the session holding that step's INPUT state
+ * (mps_state_load), mps_step_adjoint recomputes the step and replaces the
+ * seeds by the adjoint of the step's input, adding the step's terms to the
+ * gradients with respect to gravity (dim components) and kinematic
+ * viscosity; the session again holds the step's input state afterwards.
+ * Every discrete decision of the step is held fixed (neighbour sets,
+ * collision partners, order and branches, free-surface flags, the PPE
+ * unknown set, the P_min argument, ghosting); the PPE adjoint is a second
+ * ICCG solve with the step's matrix and IC(0) factor to relative residual
+ * 1e-12.  Walls, dummies and ghosts get zero adjoints.  Supported: hs_mode
+ * 0, ppe_type 0, cmps_gradient 0, no pressure clamp; other switches return
+ * MPS_ERR_UNSUPPORTED, as do more than 8 collision impulses on one
+ * particle in one step.  mps_adjoint_get reads the current seeds (NULL
+ * skips) and the accumulated gradients. */
+int  mps_state_bytes(mps_session *s, size_t *bytes);
+int  mps_state_save(mps_session *s, void *buf);
+int  mps_state_load(mps_session *s, const void *buf);
+int  mps_adjoint_seed(mps_session *s, const double *lam_pos, const double *lam_vel);
+int  mps_step_adjoint(mps_session *s);
+int  mps_adjoint_get(mps_session *s, double *lam_pos, double *lam_vel, double *grad_gravity,
+                     double *grad_viscosity);
+
 /* ---- cell sort without device allocation ------------------------------
  *
  * No counterpart in the reference (its cell list is host memory allocated

@@ -144,6 +144,12 @@ SIGNATURES = {
     "mps_reset_metrics": (I, [P]),
     "mps_run_stage": (I, [P, I, P, P, I, C.c_double]),
     "mps_cell_sort_noalloc": (I, [C.POINTER(MpsGrid), P, P, I, P, P, P, P]),
+    "mps_state_bytes": (I, [P, C.POINTER(C.c_size_t)]),
+    "mps_state_save": (I, [P, P]),
+    "mps_state_load": (I, [P, P]),
+    "mps_adjoint_seed": (I, [P, P, P]),
+    "mps_step_adjoint": (I, [P]),
+    "mps_adjoint_get": (I, [P, P, P, P, P]),
 }
 
 _lib = None

@@ -30,6 +30,7 @@
 #include "k_ops.cuh"
 #include "k_ppe.cuh"
 #include "k_sort.cuh"
+#include "k_adj.cuh"
 
 namespace mps {
 
@@ -182,6 +183,12 @@ public:
                  long long *nnz) override;
     void run_stage(int stage, const int *nb, const int *cnt, int max_nb, double arg) override;
     cudaStream_t stream() const override { return st_; }
+    size_t state_bytes() const override;
+    void state_save(void *dst) override;
+    void state_load(const void *src) override;
+    void adjoint_seed(const double *lam_pos, const double *lam_vel) override;
+    void step_adjoint() override;
+    void adjoint_get(double *lam_pos, double *lam_vel, double *grad_gravity, double *grad_viscosity) override;
 
 private:
     // ---- configuration
@@ -238,6 +245,15 @@ private:
     int pdl_mask_ = 4;
     bool ppe_valid_ = false;
 
+    // ---- differentiation form (arrays indexed by reference particle index)
+    DevArray<double> adjd_, adjsum_;
+    DevArray<int> adji_;
+    DevArray<unsigned char> snap_;           // the step's input state, for the recompute
+    Adj<D> adj_{};
+    size_t adj_cap_ = 0;
+    bool adj_rec_ = false;                   // explicit_stage records x*, u*
+    void ensure_adj();
+
     // ---- misc
     DevArray<double> vafter_, pmin_;
     DevArray<int> lptr_, lidx_, lout_, lcnt_;
@@ -279,6 +295,7 @@ private:
     void mixed_solve(int n_eq, long long nnz, bool icc);
     static constexpr int kMaxUpdates = 200;      // reliable updates of the mixed form, at most
     static constexpr double kDelta = 0.1;        // FP32 residual reduction between reliable updates
+    static constexpr double kAdjRtol = 1.0e-12;  // relative residual of the adjoint PPE solve
     int read_int(const int *dev);
     void check_err();
     void upload_list(const int *nb, const int *cnt, int max_nb);
@@ -327,7 +344,7 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
     sc_.reserve(1);
     ticket_.reserve(4);
     err_.reserve(1);
-    partials_.reserve(2 * RED_BLOCKS + 8);
+    partials_.reserve(4 * RED_BLOCKS + 8);
     MPS_CUDA(cudaMemsetAsync(ticket_.p, 0, 4 * sizeof(unsigned), st_));
     MPS_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(unsigned), st_));
 
@@ -817,6 +834,7 @@ void Engine<D>::explicit_stage(bool from_list)
     if (from_list) launch(k_viscosity<D, ListSource>, nb, TPB, 0, st_, list(), S(), k_, n, 0);
     else launch(k_viscosity<D, CellSource<D>>, nb, TPB, 0, st_, cells(), S(), k_, n, 0);
     launch(k_explicit_update<D>, nb, TPB, 0, st_, S(), k_, n);
+    if (adj_rec_) launch(k_adj_record<D>, nb, TPB, 0, st_, S(), n, adj_);
     if (k_.collision_on) {
         if (D == 3) {
             if (from_list) launch(k_collision_list<D, ListSource>, nb, TPB, 0, st_, list(), S(), k_, n, vafter_.p);
@@ -1223,6 +1241,242 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
     met.total_iterations += inner;
 }
 
+// ---- differentiation form ----------------------------------------------------
+//
+// A checkpoint is the current state buffer (positions, velocities,
+// accelerations, sort keys, pressures, densities, types, flags, reference
+// indices, cell indices) with the cell starts of its structure: everything
+// the next step reads, so that loading it and stepping reproduces the step
+// bit for bit.
+
+namespace {
+struct StateHeader {
+    long long magic, n, cap, total, dim;
+};
+constexpr long long kStateMagic = 0x4d50535354415445LL;
+}  // namespace
+
+template <int D>
+size_t Engine<D>::state_bytes() const
+{
+    size_t nd = (size_t)(4 * D + 2), ni = 5;
+    return sizeof(StateHeader) + (nd * cap_) * sizeof(double) + (ni * cap_) * sizeof(int) +
+           ((size_t)g_.total + 2) * sizeof(int);
+}
+
+template <int D>
+void Engine<D>::state_save(void *dst)
+{
+    if (!structure_) throw CudaError("no neighbour structure to checkpoint", MPS_ERR_INVALID);
+    if (!dst) throw CudaError("null checkpoint buffer", MPS_ERR_INVALID);
+    size_t nd = (size_t)(4 * D + 2), ni = 5;
+    StateHeader h{kStateMagic, n_, cap_, g_.total, D};
+    char *o = (char *)dst;
+    MPS_CUDA(cudaMemcpyAsync(o, &h, sizeof h, cudaMemcpyDefault, st_));
+    o += sizeof h;
+    MPS_CUDA(cudaMemcpyAsync(o, dbuf_[cur_].p, nd * cap_ * sizeof(double), cudaMemcpyDefault, st_));
+    o += nd * cap_ * sizeof(double);
+    MPS_CUDA(cudaMemcpyAsync(o, ibuf_[cur_].p, ni * cap_ * sizeof(int), cudaMemcpyDefault, st_));
+    o += ni * cap_ * sizeof(int);
+    MPS_CUDA(cudaMemcpyAsync(o, start_.p, ((size_t)g_.total + 2) * sizeof(int), cudaMemcpyDefault, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+}
+
+template <int D>
+void Engine<D>::state_load(const void *src)
+{
+    if (!src) throw CudaError("null checkpoint buffer", MPS_ERR_INVALID);
+    StateHeader h{};
+    MPS_CUDA(cudaMemcpyAsync(&h, src, sizeof h, cudaMemcpyDefault, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+    if (h.magic != kStateMagic || h.dim != D || h.cap != cap_ || h.total != g_.total || h.n < 0 || h.n > cap_)
+        throw CudaError("checkpoint does not belong to this session", MPS_ERR_INVALID);
+    size_t nd = (size_t)(4 * D + 2), ni = 5;
+    const char *o = (const char *)src + sizeof h;
+    MPS_CUDA(cudaMemcpyAsync(dbuf_[cur_].p, o, nd * cap_ * sizeof(double), cudaMemcpyDefault, st_));
+    o += nd * cap_ * sizeof(double);
+    MPS_CUDA(cudaMemcpyAsync(ibuf_[cur_].p, o, ni * cap_ * sizeof(int), cudaMemcpyDefault, st_));
+    o += ni * cap_ * sizeof(int);
+    MPS_CUDA(cudaMemcpyAsync(start_.p, o, ((size_t)g_.total + 2) * sizeof(int), cudaMemcpyDefault, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+    n_ = (int)h.n;
+    g_.start = start_.p;
+    structure_ = true;
+    ppe_valid_ = false;
+}
+
+template <int D>
+void Engine<D>::ensure_adj()
+{
+    if (adj_cap_ == (size_t)cap_) return;
+    size_t c = (size_t)cap_;
+    adjd_.reserve((11 * D + 5) * c + (size_t)ADJ_MAXEV * 2 * D * c);
+    adji_.reserve((2 + (size_t)ADJ_MAXEV) * c);
+    adjsum_.reserve(D + 1);
+    snap_.reserve(state_bytes());
+    double *p = adjd_.p;
+    auto take = [&](size_t m) {
+        double *r = p;
+        p += m;
+        return r;
+    };
+    for (int d = 0; d < D; d++) {
+        adj_.lx[d] = take(c);
+        adj_.lu[d] = take(c);
+        adj_.xs[d] = take(c);
+        adj_.us[d] = take(c);
+        adj_.lxc[d] = take(c);
+        adj_.luc[d] = take(c);
+        adj_.lxs[d] = take(c);
+        adj_.lus[d] = take(c);
+        adj_.lap[d] = take(c);
+        adj_.la[d] = take(c);
+        adj_.gv[d] = take(c);
+    }
+    adj_.pmv = take(c);
+    adj_.psc = take(c);
+    adj_.lp = take(c);
+    adj_.mu = take(c);
+    adj_.nv = take(c);
+    adj_.evd = take((size_t)ADJ_MAXEV * 2 * D * c);
+    adj_.pmi = adji_.p;
+    adj_.evn = adji_.p + c;
+    adj_.evj = adji_.p + 2 * c;
+    MPS_CUDA(cudaMemsetAsync(adjd_.p, 0, ((11 * D + 5) * c) * sizeof(double), st_));
+    MPS_CUDA(cudaMemsetAsync(adji_.p, 0, 2 * c * sizeof(int), st_));
+    MPS_CUDA(cudaMemsetAsync(adjsum_.p, 0, (D + 1) * sizeof(double), st_));
+    adj_cap_ = c;
+}
+
+// Seeds (host, reference order, [n][D]; null = zero) of the adjoint of the
+// state after the next step to be reversed; clears the parameter gradients.
+template <int D>
+void Engine<D>::adjoint_seed(const double *lam_pos, const double *lam_vel)
+{
+    ensure_adj();
+    int n = n_;
+    soa_in_.reserve((size_t)2 * D * cap_ + 2);
+    double *dx = lam_pos ? soa_in_.p : nullptr, *du = lam_vel ? soa_in_.p + (size_t)D * cap_ : nullptr;
+    if (lam_pos) MPS_CUDA(cudaMemcpyAsync(dx, lam_pos, sizeof(double) * D * n, cudaMemcpyHostToDevice, st_));
+    if (lam_vel) MPS_CUDA(cudaMemcpyAsync(du, lam_vel, sizeof(double) * D * n, cudaMemcpyHostToDevice, st_));
+    if (n) launch(k_adj_set<D>, nblk(n, TPB), TPB, 0, st_, n, (const double *)dx, (const double *)du, adj_);
+    MPS_CUDA(cudaMemsetAsync(adjsum_.p, 0, (D + 1) * sizeof(double), st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+    MPS_CUDA(cudaGetLastError());
+}
+
+template <int D>
+void Engine<D>::adjoint_get(double *lam_pos, double *lam_vel, double *grad_gravity, double *grad_viscosity)
+{
+    ensure_adj();
+    int n = n_;
+    soa_in_.reserve((size_t)2 * D * cap_ + 2);
+    double *dx = soa_in_.p, *du = soa_in_.p + (size_t)D * cap_;
+    if (n) launch(k_adj_get<D>, nblk(n, TPB), TPB, 0, st_, n, dx, du, adj_);
+    if (lam_pos) MPS_CUDA(cudaMemcpyAsync(lam_pos, dx, sizeof(double) * D * n, cudaMemcpyDeviceToHost, st_));
+    if (lam_vel) MPS_CUDA(cudaMemcpyAsync(lam_vel, du, sizeof(double) * D * n, cudaMemcpyDeviceToHost, st_));
+    double sums[D + 1];
+    MPS_CUDA(cudaMemcpyAsync(sums, adjsum_.p, sizeof(sums), cudaMemcpyDeviceToHost, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+    if (grad_gravity)
+        for (int d = 0; d < D; d++) grad_gravity[d] = sums[d];
+    if (grad_viscosity) *grad_viscosity = sums[D];
+}
+
+// Adjoint of one step.  The session holds the step's input state; the
+// adjoint seeds hold the adjoint of its output.  The step is recomputed
+// (recording x*, u*), its implicit part is reversed on the fresh structure
+// (correction, gradient, PPE by a second ICCG solve with the same matrix and
+// IC(0) factor, density), the input state is restored and the explicit part
+// is reversed on the previous step's structure (collision, explicit update,
+// viscosity).  Afterwards the seeds hold the adjoint of the step's input,
+// the parameter gradients have this step's terms added, and the session
+// again holds the step's input state.
+template <int D>
+void Engine<D>::step_adjoint()
+{
+    require_ref();
+    if (!structure_) throw CudaError("no neighbour structure: load a checkpoint first", MPS_ERR_INVALID);
+    if (prm_.hs_mode != 0 || prm_.ppe_type != 0 || prm_.cmps_gradient != 0 || prm_.clamp_negative_pressure ||
+        prm_.surface_tension_enabled)
+        throw CudaError("the adjoint supports hs_mode 0, ppe_type 0, cmps_gradient 0, no clamp",
+                        MPS_ERR_UNSUPPORTED);
+    ensure_adj();
+    int n = n_;
+    if (!n) return;
+    int nb = nblk(n, TPB);
+    const int RB = RED_BLOCKS;
+    state_save(snap_.p);
+    // forward recompute
+    adj_rec_ = true;
+    try {
+        explicit_stage(false);
+    } catch (...) {
+        adj_rec_ = false;
+        throw;
+    }
+    adj_rec_ = false;
+    sort();
+    launch(k_density<D, CellSource<D>>, nb, TPB, 0, st_, cells(), S(), k_, n, err_.p, 1, 1);
+    ppe(false);
+    launch(k_pmin<D, CellSource<D>>, nb, TPB, 0, st_, cells(), S(), n, pmin_.p);
+    launch(k_gradient<D, CellSource<D>>, nb, TPB, 0, st_, cells(), S(), k_, n, (const double *)pmin_.p);
+    check_err();
+    // implicit part in reverse, on the fresh structure (state before the correction)
+    launch(k_adj_seed<D>, nb, TPB, 0, st_, S(), k_, n, adj_);
+    launch(k_adj_pmin<D>, nb, TPB, 0, st_, cells(), S(), k_, n, adj_);
+    launch(k_adj_gradient<D>, nb, TPB, 0, st_, cells(), S(), k_, n, adj_);
+    MPS_CUDA(cudaMemsetAsync(adj_.mu, 0, sizeof(double) * cap_, st_));
+    int n_eq = n_eq_;
+    if (n_eq > 0) {
+        launch(k_adj_rhs, RB, CG_BLOCK, 0, st_, n_eq, (const int *)part_of_row_.p, (const int *)S().id,
+               (const double *)adj_.lp, b_.p, partials_.p, ticket_.p, sc_.p);
+        MPS_CUDA(cudaMemcpyAsync(sc_host_, sc_.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, st_));
+        MPS_CUDA(cudaStreamSynchronize(st_));
+        double bnorm = std::sqrt(sc_host_->rr_outer);
+        if (bnorm > 0.0) {
+            bool icc = prm_.solver_type == 1;
+            PcgBufs<double> v{A_.p,   F_.p,  pk_val_lo_.p, pk_val_up_.p, dinv_.p, inv_cm_.p, inv_rm_.p, x_.p,
+                              r_.p,   z_.p,  p_.p,         Ap_.p,        y_.p,    part_.p,   b_.p};
+            pcg_solve<double>(v, kAdjRtol * bnorm, prm_.cg_max_iter, icc, n_eq, nnz_);
+            launch(k_adj_mu, RB, CG_BLOCK, 0, st_, n_eq, (const int *)part_of_row_.p, (const int *)S().id,
+                   (const double *)x_.p, adj_.mu);
+        }
+    }
+    launch(k_adj_ppe_pairs<D>, nb, TPB, 0, st_, cells(), S(), k_, n, adj_, (const int *)row_of_.p);
+    // explicit part in reverse, on the previous step's structure
+    state_load(snap_.p);
+    if (k_.collision_on) {
+        if (D == 3) {
+            launch(k_adj_collision<D, true>, nb, TPB, 0, st_, cells(), S(), k_, n, adj_, err_.p);
+            launch(k_adj_collision_gather<D>, nb, TPB, 0, st_, cells(), S(), n, adj_);
+        } else {
+            // the 2-D collision runs on a structure sorted after the explicit update
+            launch(k_viscosity<D, CellSource<D>>, nb, TPB, 0, st_, cells(), S(), k_, n, 0);
+            launch(k_explicit_update<D>, nb, TPB, 0, st_, S(), k_, n);
+            sort();
+            launch(k_adj_collision<D, false>, nb, TPB, 0, st_, cells(), S(), k_, n, adj_, err_.p);
+            launch(k_adj_collision_gather<D>, nb, TPB, 0, st_, cells(), S(), n, adj_);
+            state_load(snap_.p);
+        }
+    } else {
+        launch(k_adj_no_collision<D>, nb, TPB, 0, st_, S(), n, adj_);
+    }
+    launch(k_adj_accel<D>, nb, TPB, 0, st_, S(), k_, n, adj_);
+    launch(k_adj_viscosity<D>, nb, TPB, 0, st_, cells(), S(), k_, n, adj_);
+    launch(k_adj_param_sum<D>, RB, CG_BLOCK, 0, st_, n, adj_, partials_.p, ticket_.p, adjsum_.p);
+    MPS_CUDA(cudaGetLastError());
+    unsigned e = 0;
+    MPS_CUDA(cudaMemcpyAsync(int_host_, err_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+    std::memcpy(&e, int_host_, sizeof(unsigned));
+    if (e & ERR_ADJ_EVENTS) {
+        MPS_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(unsigned), st_));
+        throw CudaError("more collision impulses on one particle than the adjoint records", MPS_ERR_UNSUPPORTED);
+    }
+    check_err();
+}
+
 // ---- introspection --------------------------------------------------------
 
 // The current structure's list into the caller's reference-layout arrays:
@@ -1594,6 +1848,28 @@ const char *mps_last_error(mps_session *s)
 int mps_run_stage(mps_session *s, int stage, const int *neighbors, const int *count, int max_nb, double arg)
 {
     MPS_API_BODY(s, s->eng->run_stage(stage, neighbors, count, max_nb, arg));
+}
+
+int mps_state_bytes(mps_session *s, size_t *bytes)
+{
+    if (!bytes) return MPS_ERR_INVALID;
+    MPS_API_BODY(s, *bytes = s->eng->state_bytes());
+}
+
+int mps_state_save(mps_session *s, void *buf) { MPS_API_BODY(s, s->eng->state_save(buf)); }
+
+int mps_state_load(mps_session *s, const void *buf) { MPS_API_BODY(s, s->eng->state_load(buf)); }
+
+int mps_adjoint_seed(mps_session *s, const double *lam_pos, const double *lam_vel)
+{
+    MPS_API_BODY(s, s->eng->adjoint_seed(lam_pos, lam_vel));
+}
+
+int mps_step_adjoint(mps_session *s) { MPS_API_BODY(s, s->eng->step_adjoint()); }
+
+int mps_adjoint_get(mps_session *s, double *lam_pos, double *lam_vel, double *grad_gravity, double *grad_viscosity)
+{
+    MPS_API_BODY(s, s->eng->adjoint_get(lam_pos, lam_vel, grad_gravity, grad_viscosity));
 }
 
 }  // extern "C"

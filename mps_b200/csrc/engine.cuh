@@ -69,6 +69,13 @@ public:
                          long long *nnz) = 0;
     virtual void run_stage(int stage, const int *nb, const int *cnt, int max_nb, double arg) = 0;
     virtual cudaStream_t stream() const = 0;
+    // differentiation form: checkpoints and the adjoint of one step
+    virtual size_t state_bytes() const = 0;
+    virtual void state_save(void *dst) = 0;
+    virtual void state_load(const void *src) = 0;
+    virtual void adjoint_seed(const double *lam_pos, const double *lam_vel) = 0;
+    virtual void step_adjoint() = 0;
+    virtual void adjoint_get(double *lam_pos, double *lam_vel, double *grad_gravity, double *grad_viscosity) = 0;
     bool profiling = false;
     mps_metrics_t met{};
     std::string last_error;

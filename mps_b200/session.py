@@ -154,6 +154,42 @@ class Session:
     def stream(self) -> int:
         return int(self.lib.mps_get_stream(self.h) or 0)
 
+    # ---- differentiation form -------------------------------------------------------
+    def state_bytes(self) -> int:
+        b = C.c_size_t()
+        self._check(self.lib.mps_state_bytes(self.h, C.byref(b)))
+        return b.value
+
+    def state_save(self, ptr: int):
+        """Checkpoint the current state into a host or device buffer of
+        state_bytes() bytes at address ``ptr``."""
+        self._check(self.lib.mps_state_save(self.h, ptr))
+
+    def state_load(self, ptr: int):
+        self._check(self.lib.mps_state_load(self.h, ptr))
+
+    def adjoint_seed(self, lam_pos=None, lam_vel=None):
+        """Adjoint of the next reversed step's output, (n, dim) arrays in
+        reference order (None = zero); clears the parameter gradients."""
+        def arr(a):
+            return None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(self.n, self.dim)
+        lx, lu = arr(lam_pos), arr(lam_vel)
+        self._check(self.lib.mps_adjoint_seed(self.h, None if lx is None else lx.ctypes.data,
+                                              None if lu is None else lu.ctypes.data))
+
+    def step_adjoint(self):
+        self._check(self.lib.mps_step_adjoint(self.h))
+
+    def adjoint_get(self):
+        """(lam_pos, lam_vel, grad_gravity, grad_viscosity)."""
+        lx = np.zeros((self.n, self.dim), dtype=np.float64)
+        lu = np.zeros((self.n, self.dim), dtype=np.float64)
+        gg = np.zeros(self.dim, dtype=np.float64)
+        gn = C.c_double()
+        self._check(self.lib.mps_adjoint_get(self.h, lx.ctypes.data, lu.ctypes.data, gg.ctypes.data,
+                                             C.byref(gn)))
+        return lx, lu, gg, gn.value
+
 
 def start(cfg, dim: int, hp: HostParticles, capacity: int | None = None, **kw) -> Session:
     """Upload, compute n0/lambda on the device, run the initial neighbour search."""
