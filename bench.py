@@ -19,7 +19,9 @@ reference compiled from source, OpenMP on all host cores, on a bounded
 sample of the same workload), `e2e` (the same metric through the C ABI with
 host buffers copied in and out every step), `clocks` (nvidia-smi sampled
 during the timed region), `gpu_launches` (kernels this library launched in
-the timed region).
+the timed region), `adjoint` (N=1: cost of the differentiation form on the
+same workload -- a short rollout's backward per step against its forward
+per step, and one isolated mps_step_adjoint).
 
 --impl reference times the reference's own CPU implementation (oracle/_ref)
 on the bounded sample, rank 0 only.
@@ -257,15 +259,20 @@ def run_b200(args, rank: int, world: int, local_rank: int):
 
     sess.close()
     e2e = None if args.no_e2e else run_e2e(wl, cfg, args, torch, dist)
+    adjoint = None
+    if world == 1 and not args.no_adjoint:
+        adjoint = run_adjoint_cost(wl, cfg, prec, torch)
 
     result = None
     if rank == 0:
         peaks, peak_kind = measured_peaks()
         nnz_mean = met["prof_nnz_sum"] / max(met["prof_iterations"], 1)
         rows_mean = met["prof_rows_sum"] / max(met["prof_iterations"], 1)
-        # SpMV algorithmic bytes per launch: A values 8 B + column 4 B per
-        # nonzero, row pointer 4 B, p 8 B, Ap 8 B per row.
-        alg_bytes = 12.0 * nnz_mean + 20.0 * rows_mean
+        # SpMV algorithmic bytes per launch: A value + column 4 B per nonzero,
+        # row pointer 4 B, p and Ap per row (values 8 B in FP64, 4 B in the
+        # mixed form's FP32 inner solve).
+        vb = 8.0 if prec == _lib.PREC_FP64 else 4.0
+        alg_bytes = (vb + 4.0) * nnz_mean + (4.0 + 2.0 * vb) * rows_mean
         spmv_ms = met["prof_spmv_ms"] / max(met["prof_spmv_launches"], 1)
         achieved = alg_bytes / (spmv_ms / 1e3) / 1e9
         peak = float(peaks.get("hbm_gbs", 6650.0))
@@ -317,12 +324,68 @@ def run_b200(args, rank: int, world: int, local_rank: int):
                          "algorithmic_bytes_per_launch": alg_bytes},
             "cpu_baseline": cpu,
             "e2e": e2e,
+            "adjoint": adjoint,
             "gpu_launches": int(launches),
             "clocks": clk,
         }
     if dist is not None:
         dist.destroy_process_group()
     return result
+
+
+def run_adjoint_cost(wl, cfg, prec, torch, steps: int = 2):
+    """Cost of the differentiation form on the same workload: a `steps`-step
+    rollout (checkpoint at its first step) forward, then its backward
+    (segment recompute from the checkpoint + one mps_step_adjoint per step,
+    each recomputing its step and reversing it), timed with CUDA events on
+    the library's stream after one untimed warm-up rollout; plus one
+    isolated state_load + mps_step_adjoint, and the device memory in use at
+    the end."""
+    import numpy as np
+
+    from mps_b200.adjoint import Rollout
+
+    roll = Rollout(cfg, 3, wl.pos, wl.types, steps, every=steps, precision=prec)
+    # one untimed forward and backward: first-use device allocations
+    xw, uw, tw = roll.forward(wl.vel, 1.0, cfg.viscosity)
+    roll.backward(np.zeros_like(xw), np.zeros_like(uw))
+    stream = torch.cuda.ExternalStream(roll.sess.stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    roll._set_params(1.0, cfg.viscosity)
+    roll._upload(wl.vel)
+    roll.sess.set_initial_params(roll.n0, roll.lam, roll.n0_count)
+    roll.sess.neighbor_search()
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    roll.ckpts = [roll._save()]
+    for _ in range(steps):
+        roll.sess.step(1)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    x, u, t = roll._final()
+    fl = (t == 0)[:, None]
+    target = wl.pos + 0.001
+    lam = 2.0 * (x - target) * fl / max(int(fl.sum()), 1)
+    ev[2].record(stream)
+    roll.backward(lam, np.zeros_like(u))
+    ev[3].record(stream)
+    torch.cuda.synchronize()
+    roll.sess.state_load(roll.ckpts[0].data_ptr())
+    ev[4].record(stream)
+    roll.sess.step_adjoint()
+    ev[5].record(stream)
+    torch.cuda.synchronize()
+    free, total = torch.cuda.mem_get_info()
+    fwd = ev[0].elapsed_time(ev[1]) / steps
+    bwd = ev[2].elapsed_time(ev[3]) / steps
+    one = ev[4].elapsed_time(ev[5])
+    roll.close()
+    return {"workload": "as config.workload", "rollout_steps": steps, "checkpoint_every": steps,
+            "fwd_ms_per_step": fwd, "backward_ms_per_step": bwd, "adjoint_over_fwd": bwd / fwd,
+            "step_adjoint_ms": one, "step_adjoint_over_fwd": one / fwd,
+            "device_memory_in_use_gb": (total - free) / 1e9,
+            "note": "backward = segment recompute + per-step recompute and reverse pass incl. the adjoint "
+                    "PPE solve; loss = mean squared distance of fluid positions to a shifted target"}
 
 
 def run_e2e(wl, cfg, args, torch, dist):
@@ -419,6 +482,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward cost measurement")
     ap.add_argument("--l0", type=float, default=None,
                     help="particle spacing override (smaller cases for profiling)")
     args = ap.parse_args()
