@@ -222,6 +222,8 @@ private:
     DevArray<double> pk_val_lo_, pk_val_up_, dinv_;
     DevArray<unsigned char> pk_k_lo_, pk_k_up_;
     DevArray<int2> adesc_;
+    DevArray<int> xlen_lo_, xlen_up_, xp_lo_, xp_up_, xc_lo_, xc_up_;   // packed cross-cell runs (CSR)
+    DevArray<double> xf_lo_, xf_up_;
     DevArray<int> inv_len_, inv_off_;        // in-cell block inverses: entries, offsets per active cell
     DevArray<double> inv_cm_, inv_rm_;       // column-major (forward) and row-major (backward) copies
     DevArray<int> colinv_, wfirst_;          // inverse offsets at colour boundaries; first cell per window
@@ -231,18 +233,19 @@ private:
     // ---- PPE
     DevArray<int> ucount_, ucol_, rs_, cell_row0_, row_of_, part_of_row_, rcount_, row_ptr_, diagpos_, col_;
     DevArray<double> A_, F_, b_, x_, r_, z_, p_, Ap_, y_, part_, partials_;
-    DevArray<float> A32_, F32_, pkv32_lo_, pkv32_up_, inv32_cm_, inv32_rm_, dinv32_;
+    DevArray<float> A32_, xf32_lo_, xf32_up_, pkv32_lo_, pkv32_up_, inv32_cm_, inv32_rm_, dinv32_;
     DevArray<float> r32_, z32_, p32_, Ap32_, y32_, part32_, d32_, zprev32_;
     DevArray<CGScalars> sc_;
     DevArray<unsigned> ticket_, err_;
     int n_eq_ = 0;
     long long nnz_ = 0;
+    int nx_lo_ = 0, nx_up_ = 0;   // entries of the packed cross-cell runs
     int ninv_ = 0;            // entries of the in-cell block inverses
     int spmv_lpr_ = 8;   // lanes per row of the CG SpMV (MPS_SPMV_LPR: 8, 16 or 32)
     int cross_lpr_ = 8;  // lanes per row of the sweeps' cross-cell products (MPS_CROSS_LPR: 4, 8, 16)
     // CG-loop kernels launched as programmatic dependents (MPS_PDL_MASK): 1 the
     // cross-cell sweep kernel, 2 the in-cell sweep kernel, 4 SpMV and vector kernels
-    int pdl_mask_ = 4;
+    int pdl_mask_ = 6;
     bool ppe_valid_ = false;
 
     // ---- differentiation form (arrays indexed by reference particle index)
@@ -285,7 +288,7 @@ private:
     void ppe(bool clamp);
     template <class T>
     struct PcgBufs {
-        const T *A, *F, *pkv_lo, *pkv_up, *dinv, *inv_cm, *inv_rm;
+        const T *A, *xf_lo, *xf_up, *pkv_lo, *pkv_up, *dinv, *inv_cm, *inv_rm;
         T *x, *r, *z, *p, *Ap, *y, *part;
         const T *b;
     };
@@ -992,6 +995,21 @@ void Engine<D>::ppe(bool clamp)
                (const int *)outpos_.p, (const int *)col_.p, (const double *)F_.p, (const int *)part_of_row_.p,
                (const int *)s.cell, (const int *)cell_row0_.p, (const int *)pk_off_lo_.p,
                (const int *)pk_off_up_.p, pk_val_lo_.p, pk_k_lo_.p, pk_val_up_.p, pk_k_up_.p, dinv_.p, err_.p);
+        // packed cross-cell runs of the factor for the sweeps
+        for (auto *v : {&xlen_lo_, &xlen_up_, &xp_lo_, &xp_up_}) v->reserve((size_t)n_eq + 1);
+        launch(k_cross_lengths, nblk(n_eq, TPB), TPB, 0, st_, n_eq, (const int *)row_ptr_.p, (const int *)inpos_.p,
+               (const int *)outpos_.p, xlen_lo_.p, xlen_up_.p);
+        scan_exclusive<int>(xlen_lo_.p, xp_lo_.p, n_eq, scanws_.p, st_);
+        scan_exclusive<int>(xlen_up_.p, xp_up_.p, n_eq, scanws_.p, st_);
+        nx_lo_ = read_int(xp_lo_.p + n_eq);
+        nx_up_ = read_int(xp_up_.p + n_eq);
+        xc_lo_.reserve((size_t)nx_lo_ + 1);
+        xf_lo_.reserve((size_t)nx_lo_ + 1);
+        xc_up_.reserve((size_t)nx_up_ + 1);
+        xf_up_.reserve((size_t)nx_up_ + 1);
+        launch(k_cross_fill, nblk(n_eq, TPB), TPB, 0, st_, n_eq, (const int *)row_ptr_.p, (const int *)inpos_.p,
+               (const int *)outpos_.p, (const int *)col_.p, (const double *)F_.p, (const int *)xp_lo_.p,
+               (const int *)xp_up_.p, xc_lo_.p, xf_lo_.p, xc_up_.p, xf_up_.p);
         int nact = act_off_[ncol];
         adesc_.reserve((size_t)nact + 1);
         if (nact)
@@ -1037,8 +1055,9 @@ void Engine<D>::ppe(bool clamp)
     if (prm_.precision == MPS_PREC_MIXED) {
         mixed_solve(n_eq, nnz, icc);
     } else {
-        PcgBufs<double> v{A_.p,   F_.p,  pk_val_lo_.p, pk_val_up_.p, dinv_.p, inv_cm_.p, inv_rm_.p, x_.p,
-                          r_.p,   z_.p,  p_.p,         Ap_.p,        y_.p,    part_.p,   b_.p};
+        PcgBufs<double> v{A_.p,         xf_lo_.p,  xf_up_.p,  pk_val_lo_.p, pk_val_up_.p, dinv_.p, inv_cm_.p,
+                          inv_rm_.p,    x_.p,      r_.p,      z_.p,         p_.p,         Ap_.p,   y_.p,
+                          part_.p,      b_.p};
         pcg_solve<double>(v, prm_.cg_tolerance, prm_.cg_max_iter, icc, n_eq, nnz);
         met.ppe_iterations = sc_host_->iter;
         met.ppe_outer = 1;
@@ -1095,12 +1114,12 @@ void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, 
             int kb = act_off_[c], ke = act_off_[c + 1];
             int rb = row_off_[c], re = row_off_[c + 1];
             if (ke <= kb) continue;
-            auto crossk = fwdir ? k_sweep_cross<true, 8, T> : k_sweep_cross<false, 8, T>;
-            if (cross_lpr_ == 4) crossk = fwdir ? k_sweep_cross<true, 4, T> : k_sweep_cross<false, 4, T>;
-            if (cross_lpr_ == 16) crossk = fwdir ? k_sweep_cross<true, 16, T> : k_sweep_cross<false, 16, T>;
-            lk(1, crossk, nblk((long long)(re - rb) * cross_lpr_, 256), 256, 0, rb, re, (const int *)row_ptr_.p,
-               (const int *)inpos_.p, (const int *)outpos_.p, (const int *)col_.p, v.F, rhs, (const T *)out, v.part,
-               (const CGScalars *)sc_.p);
+            auto crossk = k_sweep_cross<8, T>;
+            if (cross_lpr_ == 4) crossk = k_sweep_cross<4, T>;
+            if (cross_lpr_ == 16) crossk = k_sweep_cross<16, T>;
+            lk(1, crossk, nblk((long long)(re - rb) * cross_lpr_, 256), 256, 0, rb, re,
+               (const int *)(fwdir ? xp_lo_.p : xp_up_.p), (const int *)(fwdir ? xc_lo_.p : xc_up_.p),
+               fwdir ? v.xf_lo : v.xf_up, rhs, (const T *)out, v.part, (const CGScalars *)sc_.p);
             auto cellk = fwdir ? k_sweep_cell<true, T> : k_sweep_cell<false, T>;
             lk(2, cellk, nwin_[c], CELL_THREADS, sizeof(T) * CELL_STAGE, (const int *)wfirst_.p + win_off_[c],
                (const int2 *)adesc_.p, (const int *)inv_off_.p, fwdir ? v.inv_cm : v.inv_rm, pko, pkl, pkv, pkk,
@@ -1185,13 +1204,18 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
 {
     const int RB = RED_BLOCKS;
     size_t nz = (size_t)nnz;
-    for (auto *v : {&A32_, &F32_, &pkv32_lo_, &pkv32_up_}) v->reserve(nz);
+    for (auto *v : {&A32_, &pkv32_lo_, &pkv32_up_}) v->reserve(nz);
+    xf32_lo_.reserve((size_t)nx_lo_ + 1);
+    xf32_up_.reserve((size_t)nx_up_ + 1);
     for (auto *v : {&inv32_cm_, &inv32_rm_}) v->reserve((size_t)ninv_ + 1);
     for (auto *v : {&dinv32_, &r32_, &z32_, &p32_, &Ap32_, &y32_, &part32_, &d32_, &zprev32_})
         v->reserve((size_t)cap_);
     launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)A_.p, A32_.p);
     if (icc) {
-        launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)F_.p, F32_.p);
+        launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, (size_t)nx_lo_, (const double *)xf_lo_.p,
+               xf32_lo_.p);
+        launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, (size_t)nx_up_, (const double *)xf_up_.p,
+               xf32_up_.p);
         launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)pk_val_lo_.p, pkv32_lo_.p);
         launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)pk_val_up_.p, pkv32_up_.p);
         launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, (size_t)n_eq, (const double *)dinv_.p, dinv32_.p);
@@ -1211,8 +1235,9 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
     double target = std::max(prm_.cg_tolerance, rtol * bnorm);
     double rnorm = bnorm;
     int updates = 0;
-    PcgBufs<float> v{A32_.p, F32_.p,  pkv32_lo_.p, pkv32_up_.p, dinv32_.p, inv32_cm_.p, inv32_rm_.p, d32_.p,
-                     r32_.p, z32_.p,  p32_.p,      Ap32_.p,     y32_.p,    part32_.p,   r32_.p};
+    PcgBufs<float> v{A32_.p,      xf32_lo_.p, xf32_up_.p, pkv32_lo_.p, pkv32_up_.p, dinv32_.p, inv32_cm_.p,
+                     inv32_rm_.p, d32_.p,     r32_.p,     z32_.p,      p32_.p,      Ap32_.p,   y32_.p,
+                     part32_.p,   r32_.p};
     const float *zsrc = icc ? z32_.p : r32_.p;   // the preconditioned residual of the FP32 loop
     if (rnorm > target) {
         pcg_solve<float>(v, std::max(target, kDelta * rnorm), prm_.cg_max_iter, icc, n_eq, nnz);
@@ -1436,8 +1461,9 @@ void Engine<D>::step_adjoint()
         double bnorm = std::sqrt(sc_host_->rr_outer);
         if (bnorm > 0.0) {
             bool icc = prm_.solver_type == 1;
-            PcgBufs<double> v{A_.p,   F_.p,  pk_val_lo_.p, pk_val_up_.p, dinv_.p, inv_cm_.p, inv_rm_.p, x_.p,
-                              r_.p,   z_.p,  p_.p,         Ap_.p,        y_.p,    part_.p,   b_.p};
+            PcgBufs<double> v{A_.p,      xf_lo_.p, xf_up_.p, pk_val_lo_.p, pk_val_up_.p, dinv_.p, inv_cm_.p,
+                              inv_rm_.p, x_.p,     r_.p,     z_.p,         p_.p,         Ap_.p,   y_.p,
+                              part_.p,   b_.p};
             pcg_solve<double>(v, kAdjRtol * bnorm, prm_.cg_max_iter, icc, n_eq, nnz_);
             launch(k_adj_mu, RB, CG_BLOCK, 0, st_, n_eq, (const int *)part_of_row_.p, (const int *)S().id,
                    (const double *)x_.p, adj_.mu);

@@ -432,17 +432,51 @@ __global__ void k_row_splits(int n_eq, const int *__restrict__ row_ptr, const in
 //
 // k_sweep_cross: every row of a colour (rows [rbeg, rend) are contiguous)
 // sums its cross-cell run against the finished colours, LPR lanes per row,
-// into part[r] = rhs[r] - sum.
+// into part[r] = rhs[r] - sum, from the packed cross-run CSR.
 //
 // Both sweep kernels are launched as programmatic dependents (launch_pdl):
 // what they load before pdl_wait() -- row bounds, factor values and columns,
 // block inverses, cell descriptors -- is written once per step, before the
 // CG loop; x, part and the CG scalars are read only after it.
 
-template <bool FWD, int LPR, class T>
+// Cross-cell runs of the factor, packed once per step into their own CSR
+// (lo: the lower cross run [row_ptr, inpos) of every row, for the forward
+// sweep; up: the upper cross run [outpos, row_ptr+1), for the backward one)
+// so that a colour's cross entries are one contiguous stream.
+__global__ void k_cross_lengths(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ inpos,
+                                const int *__restrict__ outpos, int *__restrict__ len_lo, int *__restrict__ len_up)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_eq) return;
+    len_lo[r] = inpos[r] - row_ptr[r];
+    len_up[r] = row_ptr[r + 1] - outpos[r];
+}
+
+__global__ void k_cross_fill(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ inpos,
+                             const int *__restrict__ outpos, const int *__restrict__ col,
+                             const double *__restrict__ F, const int *__restrict__ xp_lo,
+                             const int *__restrict__ xp_up, int *__restrict__ xc_lo, double *__restrict__ xf_lo,
+                             int *__restrict__ xc_up, double *__restrict__ xf_up)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_eq) return;
+    int o = xp_lo[r];
+    for (int q = row_ptr[r]; q < inpos[r]; q++, o++) {
+        xc_lo[o] = col[q];
+        xf_lo[o] = F[q];
+    }
+    o = xp_up[r];
+    for (int q = outpos[r]; q < row_ptr[r + 1]; q++, o++) {
+        xc_up[o] = col[q];
+        xf_up[o] = F[q];
+    }
+}
+
+// part[r] = rhs[r] - sum over row r's packed cross run of F x, LPR lanes per
+// row, for the rows [rbeg, rend) of one colour.
+template <int LPR, class T>
 __global__ void __launch_bounds__(256)
-k_sweep_cross(int rbeg, int rend, const int *__restrict__ row_ptr, const int *__restrict__ inpos,
-              const int *__restrict__ outpos, const int *__restrict__ col, const T *__restrict__ F,
+k_sweep_cross(int rbeg, int rend, const int *__restrict__ xp, const int *__restrict__ xc, const T *__restrict__ xf,
               const T *rhs, const T *x, T *part, const CGScalars *sc)
 {
     constexpr int PF = 4;   // entries per lane loaded before the wait
@@ -452,8 +486,8 @@ k_sweep_cross(int rbeg, int rend, const int *__restrict__ row_ptr, const int *__
     int lane = t % LPR;
     int a = 0, b = 0;
     if (r < rend) {
-        a = FWD ? __ldg(&row_ptr[r]) : __ldg(&outpos[r]);
-        b = FWD ? __ldg(&inpos[r]) : __ldg(&row_ptr[r + 1]);
+        a = __ldg(&xp[r]);
+        b = __ldg(&xp[r + 1]);
     }
     T f[PF];
     int c[PF];
@@ -461,8 +495,8 @@ k_sweep_cross(int rbeg, int rend, const int *__restrict__ row_ptr, const int *__
     for (int u = 0; u < PF; u++) {
         int q = a + lane + u * LPR;
         bool ok = q < b;
-        f[u] = ok ? __ldg(&F[q]) : T(0);
-        c[u] = ok ? __ldg(&col[q]) : -1;
+        f[u] = ok ? __ldg(&xf[q]) : T(0);
+        c[u] = ok ? __ldg(&xc[q]) : -1;
     }
     pdl_wait();
     if (sc->done) return;
@@ -471,7 +505,7 @@ k_sweep_cross(int rbeg, int rend, const int *__restrict__ row_ptr, const int *__
     for (int u = 0; u < PF; u++)
         if (c[u] >= 0) s += f[u] * x[c[u]];
 #pragma unroll 4
-    for (int q = a + lane + PF * LPR; q < b; q += LPR) s += __ldg(&F[q]) * x[__ldg(&col[q])];
+    for (int q = a + lane + PF * LPR; q < b; q += LPR) s += __ldg(&xf[q]) * x[__ldg(&xc[q])];
 #pragma unroll
     for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LPR);
     if (lane == 0 && r < rend) part[r] = rhs[r] - s;
@@ -646,10 +680,10 @@ constexpr int MBAR_POLLS = 1 << 20;
 // that it overlaps the preceding cross-cell kernel, then its warps take the
 // window's cells in turn.
 
-constexpr int CELL_WIN = 4096;
+constexpr int CELL_WIN = 2048;
 constexpr int CELL_MAXBLK = ((SWEEP_MAXM * (SWEEP_MAXM + 1) / 2) + 3) & ~3;
 constexpr int CELL_STAGE = CELL_WIN + CELL_MAXBLK;
-constexpr int CELL_THREADS = 512;
+constexpr int CELL_THREADS = 256;
 
 // First cell of every window of one colour (cells [kbeg, kend)); entry nwin
 // is kend.  Lower bound of the window start among the cells' offsets.
@@ -688,7 +722,7 @@ __global__ void k_gather_colour_offsets(ColourIdx at, int n, const int *__restri
 // SWEEP_MAXM unknowns are solved row by row by substitution from the packed
 // runs.
 template <bool FWD, class T>
-__global__ void __launch_bounds__(CELL_THREADS, 4)
+__global__ void __launch_bounds__(CELL_THREADS, 6)
 k_sweep_cell(const int *__restrict__ wfirst, const int2 *__restrict__ desc, const int *__restrict__ inv_off,
              const T *__restrict__ inv, const int *__restrict__ pk_off, const int *__restrict__ pk_len,
              const T *__restrict__ pk_val, const unsigned char *__restrict__ pk_k, const T *__restrict__ dinv,
@@ -754,32 +788,50 @@ k_sweep_cell(const int *__restrict__ wfirst, const int2 *__restrict__ desc, cons
         int i0 = lane, i1 = lane + 32;
         T p0 = i0 < m ? part[r0 + i0] : T(0);
         T p1 = i1 < m ? part[r0 + i1] : T(0);
-        T a0 = T(0), a1 = T(0);
+        // two partial sums per row (even and odd j) halve the dependent add chain
+        T a0 = T(0), a1 = T(0), b0 = T(0), b1 = T(0);
         if (m <= 32) {
-#pragma unroll 4
-            for (int j = 0; j < m; j++) {
+#pragma unroll 2
+            for (int j = 0; j < m; j += 2) {
+                int k = j + 1;
                 T pj = __shfl_sync(0xffffffffu, p0, j);
+                T pk = __shfl_sync(0xffffffffu, p0, k & 31);
                 if (FWD) {
                     if (i0 >= j && i0 < m) a0 += blk[tri_colofs(j, m) + i0 - j] * pj;
+                    if (k < m && i0 >= k && i0 < m) b0 += blk[tri_colofs(k, m) + i0 - k] * pk;
                 } else {
                     if (i0 <= j) a0 += blk[j * (j + 1) / 2 + i0] * pj;
+                    if (k < m && i0 <= k) b0 += blk[k * (k + 1) / 2 + i0] * pk;
                 }
             }
         } else {
-#pragma unroll 2
-            for (int j = 0; j < m; j++) {
+            for (int j = 0; j < m; j += 2) {
+                int k = j + 1;
                 T pj = __shfl_sync(0xffffffffu, j < 32 ? p0 : p1, j & 31);
+                T pk = __shfl_sync(0xffffffffu, k < 32 ? p0 : p1, k & 31);
                 if (FWD) {
                     const T *cj = blk + tri_colofs(j, m) - j;
                     if (i0 >= j) a0 += cj[i0] * pj;
                     if (i1 >= j && i1 < m) a1 += cj[i1] * pj;
+                    if (k < m) {
+                        const T *ck = blk + tri_colofs(k, m) - k;
+                        if (i0 >= k) b0 += ck[i0] * pk;
+                        if (i1 >= k && i1 < m) b1 += ck[i1] * pk;
+                    }
                 } else {
                     const T *rj = blk + j * (j + 1) / 2;
                     if (i0 <= j) a0 += rj[i0] * pj;
                     if (i1 <= j) a1 += rj[i1] * pj;
+                    if (k < m) {
+                        const T *rk = blk + k * (k + 1) / 2;
+                        if (i0 <= k) b0 += rk[i0] * pk;
+                        if (i1 <= k) b1 += rk[i1] * pk;
+                    }
                 }
             }
         }
+        a0 += b0;
+        a1 += b1;
         if (i0 < m) x[r0 + i0] = a0;
         if (i1 < m) x[r0 + i1] = a1;
     }
