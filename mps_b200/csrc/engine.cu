@@ -246,6 +246,7 @@ private:
     // CG-loop kernels launched as programmatic dependents (MPS_PDL_MASK): 1 the
     // cross-cell sweep kernel, 2 the in-cell sweep kernel, 4 SpMV and vector kernels
     int pdl_mask_ = 6;
+    int cell_win_ = CELL_WIN;   // entries per window of the staged in-cell sweep (MPS_CELL_WIN: 1024..4096)
     bool ppe_valid_ = false;
 
     // ---- differentiation form (arrays indexed by reference particle index)
@@ -326,6 +327,10 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
         if (v == 8 || v == 16 || v == 32) spmv_lpr_ = v;
     }
     if (const char *e = std::getenv("MPS_PDL_MASK")) pdl_mask_ = std::atoi(e) & 7;
+    if (const char *e = std::getenv("MPS_CELL_WIN")) {
+        int v = std::atoi(e);
+        if (v >= 1024 && v <= CELL_WIN_MAX && v % 4 == 0) cell_win_ = v;
+    }
     if (const char *e = std::getenv("MPS_CROSS_LPR")) {
         int v = std::atoi(e);
         if (v == 4 || v == 8 || v == 16) cross_lpr_ = v;
@@ -338,9 +343,9 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
     MPS_CUDA(cudaMallocHost((void **)&int_host_, 64 * sizeof(int)));
     // the staged in-cell sweeps take more than the default 48 KB of dynamic shared memory
     MPS_CUDA(cudaFuncSetAttribute(k_sweep_cell<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(sizeof(double) * CELL_STAGE)));
+                                  (int)(sizeof(double) * CELL_STAGE_MAX)));
     MPS_CUDA(cudaFuncSetAttribute(k_sweep_cell<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(sizeof(double) * CELL_STAGE)));
+                                  (int)(sizeof(double) * CELL_STAGE_MAX)));
     alloc_state();
     build_grid();
     compute_consts();
@@ -1033,7 +1038,7 @@ void Engine<D>::ppe(bool clamp)
         nwin_.assign(ncol, 0);
         for (int c = 0; c < ncol; c++) {
             int span = int_host_[c + 1] - int_host_[c];
-            nwin_[c] = act_off_[c + 1] > act_off_[c] ? std::max(1, (span + CELL_WIN - 1) / CELL_WIN) : 0;
+            nwin_[c] = act_off_[c + 1] > act_off_[c] ? std::max(1, (span + cell_win_ - 1) / cell_win_) : 0;
             win_off_[c + 1] = win_off_[c] + nwin_[c] + 1;
         }
         inv_cm_.reserve((size_t)ninv + 1);
@@ -1048,7 +1053,7 @@ void Engine<D>::ppe(bool clamp)
         for (int c = 0; c < ncol; c++)
             if (nwin_[c])
                 launch(k_inv_windows, nblk(nwin_[c] + 1, TPB), TPB, 0, st_, act_off_[c], act_off_[c + 1],
-                       (const int *)inv_off_.p, nwin_[c], wfirst_.p + win_off_[c]);
+                       (const int *)inv_off_.p, cell_win_, nwin_[c], wfirst_.p + win_off_[c]);
     }
     MPS_CUDA(cudaEventRecord(ev_[3], st_));
 
@@ -1121,9 +1126,10 @@ void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, 
                (const int *)(fwdir ? xp_lo_.p : xp_up_.p), (const int *)(fwdir ? xc_lo_.p : xc_up_.p),
                fwdir ? v.xf_lo : v.xf_up, rhs, (const T *)out, v.part, (const CGScalars *)sc_.p);
             auto cellk = fwdir ? k_sweep_cell<true, T> : k_sweep_cell<false, T>;
-            lk(2, cellk, nwin_[c], CELL_THREADS, sizeof(T) * CELL_STAGE, (const int *)wfirst_.p + win_off_[c],
+            lk(2, cellk, nwin_[c], CELL_THREADS, sizeof(T) * (cell_win_ + CELL_MAXBLK),
+               (const int *)wfirst_.p + win_off_[c],
                (const int2 *)adesc_.p, (const int *)inv_off_.p, fwdir ? v.inv_cm : v.inv_rm, pko, pkl, pkv, pkk,
-               v.dinv, (const T *)v.part, out, (const CGScalars *)sc_.p, err_.p);
+               v.dinv, (const T *)v.part, out, (const CGScalars *)sc_.p, cell_win_ + CELL_MAXBLK, err_.p);
         }
     };
     auto spmv = [&]() {

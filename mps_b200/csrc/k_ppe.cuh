@@ -675,19 +675,21 @@ constexpr int MBAR_POLLS = 1 << 20;
 // The cells of one colour are consecutive in the block-inverse arrays, so a
 // colour splits into windows of CELL_WIN entries: window w holds the cells
 // whose blocks start in [w CELL_WIN, (w+1) CELL_WIN) of the colour's range,
-// one contiguous run of at most CELL_STAGE entries.  A CTA per window copies
+// one contiguous run of at most win + CELL_MAXBLK entries (the stage).  A CTA per window copies
 // its run into shared memory with one bulk copy, issued before pdl_wait() so
 // that it overlaps the preceding cross-cell kernel, then its warps take the
 // window's cells in turn.
 
-constexpr int CELL_WIN = 2048;
+constexpr int CELL_WIN = 1024;        // default window (entries); MPS_CELL_WIN selects 1024..4096
+constexpr int CELL_WIN_MAX = 4096;
 constexpr int CELL_MAXBLK = ((SWEEP_MAXM * (SWEEP_MAXM + 1) / 2) + 3) & ~3;
-constexpr int CELL_STAGE = CELL_WIN + CELL_MAXBLK;
+constexpr int CELL_STAGE_MAX = CELL_WIN_MAX + CELL_MAXBLK;
 constexpr int CELL_THREADS = 256;
 
 // First cell of every window of one colour (cells [kbeg, kend)); entry nwin
 // is kend.  Lower bound of the window start among the cells' offsets.
-__global__ void k_inv_windows(int kbeg, int kend, const int *__restrict__ inv_off, int nwin, int *__restrict__ wfirst)
+__global__ void k_inv_windows(int kbeg, int kend, const int *__restrict__ inv_off, int win, int nwin,
+                              int *__restrict__ wfirst)
 {
     int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w > nwin) return;
@@ -695,7 +697,7 @@ __global__ void k_inv_windows(int kbeg, int kend, const int *__restrict__ inv_of
         wfirst[w] = kend;
         return;
     }
-    int target = inv_off[kbeg] + w * CELL_WIN;
+    int target = inv_off[kbeg] + w * win;
     int lo = kbeg, hi = kend;
     while (lo < hi) {
         int mid = (lo + hi) >> 1;
@@ -726,7 +728,7 @@ __global__ void __launch_bounds__(CELL_THREADS, 6)
 k_sweep_cell(const int *__restrict__ wfirst, const int2 *__restrict__ desc, const int *__restrict__ inv_off,
              const T *__restrict__ inv, const int *__restrict__ pk_off, const int *__restrict__ pk_len,
              const T *__restrict__ pk_val, const unsigned char *__restrict__ pk_k, const T *__restrict__ dinv,
-             const T *part, T *x, const CGScalars *sc, unsigned *err)
+             const T *part, T *x, const CGScalars *sc, int stage_elems, unsigned *err)
 {
     extern __shared__ __align__(128) unsigned char cell_stage[];
     __shared__ __align__(8) unsigned long long bar;
@@ -738,7 +740,7 @@ k_sweep_cell(const int *__restrict__ wfirst, const int2 *__restrict__ desc, cons
         o0 = __ldg(&inv_off[ka]);
         nel = __ldg(&inv_off[kb]) - o0;
     }
-    bool staged = nel > 0 && nel <= CELL_STAGE;
+    bool staged = nel > 0 && nel <= stage_elems;
     unsigned b = smem_u32(&bar);
     if (threadIdx.x == 0 && staged) mbar_init(b, 1);
     __syncthreads();
@@ -761,7 +763,7 @@ k_sweep_cell(const int *__restrict__ wfirst, const int2 *__restrict__ desc, cons
         mbar_wait(b, 0, MBAR_POLLS);
         return;
     }
-    if (nel > CELL_STAGE && threadIdx.x == 0) atomicOr(err, ERR_WINDOW_OVERFLOW);
+    if (nel > stage_elems && threadIdx.x == 0) atomicOr(err, ERR_WINDOW_OVERFLOW);
     if (sc->done) return;
     const T *src = staged ? stage : inv + o0;
     for (; k < kb; k += CELL_THREADS / 32) {
