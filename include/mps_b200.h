@@ -75,14 +75,23 @@ typedef struct {
     int    use_analytical_lambda;
     int    hs_mode;
     int    precision;                 /* MPS_PREC_* */
-    double refine_tolerance;          /* mixed form: inner FP32 relative tolerance */
+    double refine_tolerance;          /* mixed form: stop at ||b - A x|| <= max(cg_tolerance,
+                                         refine_tolerance * ||b||) (0 = 1e-10) */
+    /* Driven walls (no counterpart in the reference, whose walls never move):
+     * every WALL and DUMMY particle follows x_axis = rest + A sin(2 pi f t),
+     * u_axis = 2 pi f A cos(2 pi f t), rest = its position at upload, t the
+     * session time (steps taken x dt).  A = 0 is the reference's fixed walls,
+     * bit for bit. */
+    double wall_drive_amp;            /* A (m) */
+    double wall_drive_freq;           /* f (Hz) */
+    int    wall_drive_axis;           /* 0 = x, 1 = y, 2 = z */
 } mps_params_t;
 
 /* Per-step metrics (the reference computes and discards its iteration count,
  * pressure_solver.c:553-561). */
 typedef struct {
     int    ppe_iterations;            /* CG iterations of the last step (inner, summed) */
-    int    ppe_outer;                 /* refinement sweeps (mixed form), else 1 */
+    int    ppe_outer;                 /* reliable updates (mixed form), else 1 */
     double ppe_residual;              /* final recursive residual norm */
     int    n_eq;
     long long nnz;
@@ -233,14 +242,15 @@ int  mps_run_stage(mps_session *s, int stage, const int *neighbors, const int *c
  * 0, ppe_type 0, cmps_gradient 0, no pressure clamp; other switches return
  * MPS_ERR_UNSUPPORTED, as do more than 8 collision impulses on one
  * particle in one step.  mps_adjoint_get reads the current seeds (NULL
- * skips) and the accumulated gradients. */
+ * skips) and the accumulated gradients; grad_drive receives the gradients
+ * with respect to the wall drive's amplitude and frequency (2 doubles). */
 int  mps_state_bytes(mps_session *s, size_t *bytes);
 int  mps_state_save(mps_session *s, void *buf);
 int  mps_state_load(mps_session *s, const void *buf);
 int  mps_adjoint_seed(mps_session *s, const double *lam_pos, const double *lam_vel);
 int  mps_step_adjoint(mps_session *s);
 int  mps_adjoint_get(mps_session *s, double *lam_pos, double *lam_vel, double *grad_gravity,
-                     double *grad_viscosity);
+                     double *grad_viscosity, double *grad_drive);
 
 /* ---- cell sort without device allocation ------------------------------
  *

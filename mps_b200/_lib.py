@@ -71,6 +71,9 @@ class MpsParams(C.Structure):
         ("hs_mode", C.c_int),
         ("precision", C.c_int),
         ("refine_tolerance", C.c_double),
+        ("wall_drive_amp", C.c_double),
+        ("wall_drive_freq", C.c_double),
+        ("wall_drive_axis", C.c_int),
     ]
 
 
@@ -149,7 +152,7 @@ SIGNATURES = {
     "mps_state_load": (I, [P, P]),
     "mps_adjoint_seed": (I, [P, P, P]),
     "mps_step_adjoint": (I, [P]),
-    "mps_adjoint_get": (I, [P, P, P, P, P]),
+    "mps_adjoint_get": (I, [P, P, P, P, P, P]),
 }
 
 _lib = None

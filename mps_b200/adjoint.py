@@ -3,9 +3,10 @@ function for ``torch.autograd``, over the session C ABI.
 
 ``Rollout(cfg, dim, pos, types, steps, every)`` binds one session to a fixed
 initial geometry; calling it with an initial velocity field ``u0`` (n, dim),
-a gravity scale and a kinematic viscosity (torch FP64 tensors) runs
-``steps`` device-resident time steps and returns the final positions and
-velocities (n, dim) in reference order.  Backward runs the hand-written
+a gravity scale, a kinematic viscosity and, for driven walls, the drive's
+amplitude and frequency (torch FP64 tensors) runs ``steps`` device-resident
+time steps and returns the final positions and velocities (n, dim) in
+reference order.  Backward runs the hand-written
 adjoint kernels of the library (``mps_step_adjoint``) from the last step to
 the first with checkpoint-every-k recomputation: the forward saves the
 state every ``every`` steps; the backward reloads each checkpoint, recomputes
@@ -31,7 +32,7 @@ from .types import HostParticles
 
 class Rollout:
     def __init__(self, cfg, dim: int, pos, types, steps: int, every: int = 1, precision: int = _lib.PREC_FP64,
-                 checkpoint_device: str | None = None):
+                 checkpoint_device: str | None = None, drive_axis: int = 0):
         if steps < 1 or every < 1:
             raise ValueError("steps and every must be positive")
         self.cfg, self.dim, self.steps, self.every = cfg, dim, int(steps), int(every)
@@ -40,6 +41,7 @@ class Rollout:
         self.n = self.types.shape[0]
         self.sess = Session(cfg, dim, self.n, precision=precision)
         self.g_base = np.array([cfg.gravity[d] for d in range(dim)], dtype=np.float64)
+        self.drive_axis = int(drive_axis)
         self._upload(np.zeros_like(self.pos))
         self.n0, self.lam, self.n0_count = self.sess.compute_initial_params()
         self.nbytes = self.sess.state_bytes()
@@ -52,11 +54,14 @@ class Rollout:
         hp = HostParticles(self.dim, self.pos, u0, self.types)
         self.sess.upload(hp)
 
-    def _set_params(self, gscale: float, nu: float):
+    def _set_params(self, gscale: float, nu: float, amp: float = 0.0, freq: float = 0.0):
         p = self.sess.params
         for d in range(self.dim):
             p.gravity[d] = float(self.g_base[d] * gscale)
         p.viscosity = float(nu)
+        p.wall_drive_amp = float(amp)
+        p.wall_drive_freq = float(freq)
+        p.wall_drive_axis = self.drive_axis
         self.sess._check(self.sess.lib.mps_update_params(self.sess.h, p))
 
     def _buffer(self) -> torch.Tensor:
@@ -72,9 +77,9 @@ class Rollout:
         return out["pos"].copy(), out["vel"].copy(), out["type"].copy()
 
     # ---- forward / backward ---------------------------------------------------------
-    def forward(self, u0: np.ndarray, gscale: float, nu: float):
+    def forward(self, u0: np.ndarray, gscale: float, nu: float, amp: float = 0.0, freq: float = 0.0):
         """Run the rollout; returns (x_T, u_T, types_T) and keeps the checkpoints."""
-        self._set_params(gscale, nu)
+        self._set_params(gscale, nu, amp, freq)
         self._upload(u0)
         self.sess.set_initial_params(self.n0, self.lam, self.n0_count)
         self.sess.neighbor_search()
@@ -87,7 +92,8 @@ class Rollout:
 
     def backward(self, lam_x: np.ndarray, lam_u: np.ndarray):
         """Adjoint of the last forward run from the adjoint of (x_T, u_T):
-        returns (dL/dx_0, dL/du_0, dL/d gravity_scale, dL/d viscosity)."""
+        returns (dL/dx_0, dL/du_0, dL/d gravity_scale, dL/d viscosity,
+        dL/d drive amplitude, dL/d drive frequency)."""
         self.sess.adjoint_seed(lam_x, lam_u)
         nseg = len(self.ckpts)
         for seg in reversed(range(nseg)):
@@ -101,20 +107,22 @@ class Rollout:
             for k in reversed(range(s1 - s0)):
                 self.sess.state_load(states[k].data_ptr())
                 self.sess.step_adjoint()
-        lx, lu, gg, gn = self.sess.adjoint_get()
-        return lx, lu, float(np.dot(gg, self.g_base)), gn
+        lx, lu, gg, gn, gd = self.sess.adjoint_get()
+        return lx, lu, float(np.dot(gg, self.g_base)), gn, float(gd[0]), float(gd[1])
 
     def close(self):
         self.sess.close()
 
-    def __call__(self, u0: torch.Tensor, gscale: torch.Tensor, nu: torch.Tensor):
-        return _RolloutFn.apply(u0, gscale, nu, self)
+    def __call__(self, u0: torch.Tensor, gscale: torch.Tensor, nu: torch.Tensor, amp: torch.Tensor | None = None,
+                 freq: torch.Tensor | None = None):
+        z = torch.zeros((), dtype=torch.float64, device=u0.device)
+        return _RolloutFn.apply(u0, gscale, nu, z if amp is None else amp, z if freq is None else freq, self)
 
 
 class _RolloutFn(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, u0, gscale, nu, roll):
-        x, u, t = roll.forward(u0.detach().cpu().numpy(), float(gscale), float(nu))
+    def forward(ctx, u0, gscale, nu, amp, freq, roll):
+        x, u, t = roll.forward(u0.detach().cpu().numpy(), float(gscale), float(nu), float(amp), float(freq))
         ctx.roll = roll
         ctx.dev = u0.device
         return (torch.from_numpy(x).to(ctx.dev), torch.from_numpy(u).to(ctx.dev))
@@ -124,6 +132,7 @@ class _RolloutFn(torch.autograd.Function):
         roll = ctx.roll
         lx = np.zeros((roll.n, roll.dim)) if gx is None else gx.detach().cpu().numpy()
         lu = np.zeros((roll.n, roll.dim)) if gu is None else gu.detach().cpu().numpy()
-        _, du0, dgs, dnu = roll.backward(lx, lu)
+        _, du0, dgs, dnu, da, df = roll.backward(lx, lu)
         f64 = dict(dtype=torch.float64, device=ctx.dev)
-        return torch.from_numpy(du0).to(ctx.dev), torch.tensor(dgs, **f64), torch.tensor(dnu, **f64), None
+        return (torch.from_numpy(du0).to(ctx.dev), torch.tensor(dgs, **f64), torch.tensor(dnu, **f64),
+                torch.tensor(da, **f64), torch.tensor(df, **f64), None)

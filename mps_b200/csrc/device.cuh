@@ -116,6 +116,7 @@ struct Consts {
     int    max_nb;
     int    ppe_type, hs_mode, cmps, surf_method, clamp;
     int    collision_on;
+    int    drive_on, drive_axis;   // driven walls (A != 0) and their axis
 };
 
 // Structure-of-arrays particle state.  `key` holds the positions at the

@@ -188,7 +188,8 @@ public:
     void state_load(const void *src) override;
     void adjoint_seed(const double *lam_pos, const double *lam_vel) override;
     void step_adjoint() override;
-    void adjoint_get(double *lam_pos, double *lam_vel, double *grad_gravity, double *grad_viscosity) override;
+    void adjoint_get(double *lam_pos, double *lam_vel, double *grad_gravity, double *grad_viscosity,
+                     double *grad_drive) override;
 
 private:
     // ---- configuration
@@ -248,6 +249,11 @@ private:
     int pdl_mask_ = 6;
     int cell_win_ = CELL_WIN;   // entries per window of the staged in-cell sweep (MPS_CELL_WIN: 1024..4096)
     bool ppe_valid_ = false;
+
+    // ---- driven walls
+    long long tstep_ = 0;                    // steps taken since the last upload (time = tstep_ dt)
+    DevArray<double> rest_;                  // rest positions at upload, [axis][reference index]
+    void drive_terms(double t, double *dx, double *vel) const;
 
     // ---- differentiation form (arrays indexed by reference particle index)
     DevArray<double> adjd_, adjsum_;
@@ -320,6 +326,7 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
     if (p.dim != D) throw CudaError("dimension mismatch", MPS_ERR_INVALID);
     if (capacity <= 0) throw CudaError("capacity must be positive", MPS_ERR_INVALID);
     if (p.surface_tension_enabled) throw CudaError("surface tension is not on this path", MPS_ERR_UNSUPPORTED);
+    if (p.wall_drive_axis < 0 || p.wall_drive_axis >= D) throw CudaError("wall_drive_axis out of range", MPS_ERR_INVALID);
     cap_ = capacity;
     prm_ = p;
     if (const char *e = std::getenv("MPS_SPMV_LPR")) {
@@ -352,7 +359,7 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
     sc_.reserve(1);
     ticket_.reserve(4);
     err_.reserve(1);
-    partials_.reserve(4 * RED_BLOCKS + 8);
+    partials_.reserve(6 * RED_BLOCKS + 8);
     MPS_CUDA(cudaMemsetAsync(ticket_.p, 0, 4 * sizeof(unsigned), st_));
     MPS_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(unsigned), st_));
 
@@ -426,6 +433,7 @@ void Engine<D>::alloc_state()
     where_.reserve(cap_);
     vafter_.reserve((size_t)D * cap_);
     pmin_.reserve(cap_);
+    rest_.reserve((size_t)D * cap_);
     row_of_.reserve(cap_);
     part_of_row_.reserve(cap_);
     rcount_.reserve(cap_ + 1);
@@ -541,6 +549,8 @@ void Engine<D>::compute_consts()
     k.surf_method = p.surface_detection_method;
     k.clamp = p.clamp_negative_pressure;
     k.collision_on = (D == 2) ? 1 : (p.collision_distance_ratio > 0.0);
+    k.drive_on = p.wall_drive_amp != 0.0;
+    k.drive_axis = p.wall_drive_axis;
 }
 
 template <int D>
@@ -548,6 +558,7 @@ void Engine<D>::update_params(const mps_params_t &p)
 {
     if (p.dim != D) throw CudaError("dimension mismatch", MPS_ERR_INVALID);
     if (p.surface_tension_enabled) throw CudaError("surface tension is not on this path", MPS_ERR_UNSUPPORTED);
+    if (p.wall_drive_axis < 0 || p.wall_drive_axis >= D) throw CudaError("wall_drive_axis out of range", MPS_ERR_INVALID);
     bool regrid = false;
     for (int d = 0; d < D; d++)
         regrid |= p.domain_min[d] != prm_.domain_min[d] || p.domain_max[d] != prm_.domain_max[d];
@@ -600,8 +611,10 @@ void Engine<D>::upload_aos(const void *aos, int num)
     aos_.reserve(bytes + 8);
     MPS_CUDA(cudaMemcpyAsync(aos_.p, aos, bytes, cudaMemcpyHostToDevice, st_));
     if (num) launch(k_unpack<D>, nblk(num, TPB), TPB, 0, st_, aos_.p, S(), num);
+    if (num) launch(k_set_rest<D>, nblk(num, TPB), TPB, 0, st_, S(), num, cap_, rest_.p);
     MPS_CUDA(cudaGetLastError());
     MPS_CUDA(cudaStreamSynchronize(st_));
+    tstep_ = 0;
     structure_ = false;
     ppe_valid_ = false;
 }
@@ -632,8 +645,10 @@ void Engine<D>::upload_soa(const double *pos, const double *vel, const int *type
     if (num)
         launch(k_unpack_soa<D>, nblk(num, TPB), TPB, 0, st_, soa_in_.p, soa_in_.p + (size_t)D * num, int_in_.p, S(),
                                                          num);
+    if (num) launch(k_set_rest<D>, nblk(num, TPB), TPB, 0, st_, S(), num, cap_, rest_.p);
     MPS_CUDA(cudaGetLastError());
     MPS_CUDA(cudaStreamSynchronize(st_));
+    tstep_ = 0;
     structure_ = false;
     ppe_valid_ = false;
 }
@@ -842,6 +857,12 @@ void Engine<D>::explicit_stage(bool from_list)
     if (from_list) launch(k_viscosity<D, ListSource>, nb, TPB, 0, st_, list(), S(), k_, n, 0);
     else launch(k_viscosity<D, CellSource<D>>, nb, TPB, 0, st_, cells(), S(), k_, n, 0);
     launch(k_explicit_update<D>, nb, TPB, 0, st_, S(), k_, n);
+    if (k_.drive_on) {
+        double dx, vel;
+        drive_terms((double)(tstep_ + 1) * prm_.dt, &dx, &vel);
+        launch(k_drive_walls<D>, nb, TPB, 0, st_, S(), n, (const double *)rest_.p + (size_t)k_.drive_axis * cap_,
+               k_.drive_axis, dx, vel);
+    }
     if (adj_rec_) launch(k_adj_record<D>, nb, TPB, 0, st_, S(), n, adj_);
     if (k_.collision_on) {
         if (D == 3) {
@@ -895,6 +916,7 @@ void Engine<D>::step(int nsteps)
         met.ms_factor = t23;
         met.ms_solve = t34;
         met.total_steps++;
+        tstep_++;
     }
 }
 
@@ -910,6 +932,7 @@ void Engine<D>::step_with_list(const int *nb, const int *cnt, int max_nb)
     MPS_CUDA(cudaEventRecord(ev_[5], st_));
     check_err();
     met.total_steps++;
+    tstep_++;
 }
 
 // ---- PPE ------------------------------------------------------------------------
@@ -1280,9 +1303,20 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
 // the next step reads, so that loading it and stepping reproduces the step
 // bit for bit.
 
+// Drive values at time t: displacement A sin(w t) and velocity A w cos(w t),
+// w = 2 pi f (the oracle's oracle_wall_drive_terms, the same expressions).
+template <int D>
+void Engine<D>::drive_terms(double t, double *dx, double *vel) const
+{
+    double w = 2.0 * 3.14159265358979323846 * prm_.wall_drive_freq;
+    double ph = w * t;
+    *dx = prm_.wall_drive_amp * std::sin(ph);
+    *vel = prm_.wall_drive_amp * w * std::cos(ph);
+}
+
 namespace {
 struct StateHeader {
-    long long magic, n, cap, total, dim;
+    long long magic, n, cap, total, dim, tstep;
 };
 constexpr long long kStateMagic = 0x4d50535354415445LL;
 }  // namespace
@@ -1301,7 +1335,7 @@ void Engine<D>::state_save(void *dst)
     if (!structure_) throw CudaError("no neighbour structure to checkpoint", MPS_ERR_INVALID);
     if (!dst) throw CudaError("null checkpoint buffer", MPS_ERR_INVALID);
     size_t nd = (size_t)(4 * D + 2), ni = 5;
-    StateHeader h{kStateMagic, n_, cap_, g_.total, D};
+    StateHeader h{kStateMagic, n_, cap_, g_.total, D, tstep_};
     char *o = (char *)dst;
     MPS_CUDA(cudaMemcpyAsync(o, &h, sizeof h, cudaMemcpyDefault, st_));
     o += sizeof h;
@@ -1331,6 +1365,7 @@ void Engine<D>::state_load(const void *src)
     MPS_CUDA(cudaMemcpyAsync(start_.p, o, ((size_t)g_.total + 2) * sizeof(int), cudaMemcpyDefault, st_));
     MPS_CUDA(cudaStreamSynchronize(st_));
     n_ = (int)h.n;
+    tstep_ = h.tstep;
     g_.start = start_.p;
     structure_ = true;
     ppe_valid_ = false;
@@ -1341,9 +1376,9 @@ void Engine<D>::ensure_adj()
 {
     if (adj_cap_ == (size_t)cap_) return;
     size_t c = (size_t)cap_;
-    adjd_.reserve((11 * D + 5) * c + (size_t)ADJ_MAXEV * 2 * D * c);
+    adjd_.reserve((11 * D + 7) * c + (size_t)ADJ_MAXEV * 2 * D * c);
     adji_.reserve((2 + (size_t)ADJ_MAXEV) * c);
-    adjsum_.reserve(D + 1);
+    adjsum_.reserve(D + 3);
     snap_.reserve(state_bytes());
     double *p = adjd_.p;
     auto take = [&](size_t m) {
@@ -1369,13 +1404,15 @@ void Engine<D>::ensure_adj()
     adj_.lp = take(c);
     adj_.mu = take(c);
     adj_.nv = take(c);
+    adj_.dA = take(c);
+    adj_.df = take(c);
     adj_.evd = take((size_t)ADJ_MAXEV * 2 * D * c);
     adj_.pmi = adji_.p;
     adj_.evn = adji_.p + c;
     adj_.evj = adji_.p + 2 * c;
-    MPS_CUDA(cudaMemsetAsync(adjd_.p, 0, ((11 * D + 5) * c) * sizeof(double), st_));
+    MPS_CUDA(cudaMemsetAsync(adjd_.p, 0, ((11 * D + 7) * c) * sizeof(double), st_));
     MPS_CUDA(cudaMemsetAsync(adji_.p, 0, 2 * c * sizeof(int), st_));
-    MPS_CUDA(cudaMemsetAsync(adjsum_.p, 0, (D + 1) * sizeof(double), st_));
+    MPS_CUDA(cudaMemsetAsync(adjsum_.p, 0, (D + 3) * sizeof(double), st_));
     adj_cap_ = c;
 }
 
@@ -1391,13 +1428,14 @@ void Engine<D>::adjoint_seed(const double *lam_pos, const double *lam_vel)
     if (lam_pos) MPS_CUDA(cudaMemcpyAsync(dx, lam_pos, sizeof(double) * D * n, cudaMemcpyHostToDevice, st_));
     if (lam_vel) MPS_CUDA(cudaMemcpyAsync(du, lam_vel, sizeof(double) * D * n, cudaMemcpyHostToDevice, st_));
     if (n) launch(k_adj_set<D>, nblk(n, TPB), TPB, 0, st_, n, (const double *)dx, (const double *)du, adj_);
-    MPS_CUDA(cudaMemsetAsync(adjsum_.p, 0, (D + 1) * sizeof(double), st_));
+    MPS_CUDA(cudaMemsetAsync(adjsum_.p, 0, (D + 3) * sizeof(double), st_));
     MPS_CUDA(cudaStreamSynchronize(st_));
     MPS_CUDA(cudaGetLastError());
 }
 
 template <int D>
-void Engine<D>::adjoint_get(double *lam_pos, double *lam_vel, double *grad_gravity, double *grad_viscosity)
+void Engine<D>::adjoint_get(double *lam_pos, double *lam_vel, double *grad_gravity, double *grad_viscosity,
+                            double *grad_drive)
 {
     ensure_adj();
     int n = n_;
@@ -1406,12 +1444,16 @@ void Engine<D>::adjoint_get(double *lam_pos, double *lam_vel, double *grad_gravi
     if (n) launch(k_adj_get<D>, nblk(n, TPB), TPB, 0, st_, n, dx, du, adj_);
     if (lam_pos) MPS_CUDA(cudaMemcpyAsync(lam_pos, dx, sizeof(double) * D * n, cudaMemcpyDeviceToHost, st_));
     if (lam_vel) MPS_CUDA(cudaMemcpyAsync(lam_vel, du, sizeof(double) * D * n, cudaMemcpyDeviceToHost, st_));
-    double sums[D + 1];
+    double sums[D + 3];
     MPS_CUDA(cudaMemcpyAsync(sums, adjsum_.p, sizeof(sums), cudaMemcpyDeviceToHost, st_));
     MPS_CUDA(cudaStreamSynchronize(st_));
     if (grad_gravity)
         for (int d = 0; d < D; d++) grad_gravity[d] = sums[d];
     if (grad_viscosity) *grad_viscosity = sums[D];
+    if (grad_drive) {
+        grad_drive[0] = sums[D + 1];
+        grad_drive[1] = sums[D + 2];
+    }
 }
 
 // Adjoint of one step.  The session holds the step's input state; the
@@ -1496,6 +1538,20 @@ void Engine<D>::step_adjoint()
     }
     launch(k_adj_accel<D>, nb, TPB, 0, st_, S(), k_, n, adj_);
     launch(k_adj_viscosity<D>, nb, TPB, 0, st_, cells(), S(), k_, n, adj_);
+    {
+        DriveT dv{};
+        dv.A = prm_.wall_drive_amp;
+        dv.w = 2.0 * 3.14159265358979323846 * prm_.wall_drive_freq;
+        dv.t0 = (double)tstep_ * prm_.dt;
+        dv.t1 = (double)(tstep_ + 1) * prm_.dt;
+        dv.s0 = std::sin(dv.w * dv.t0);
+        dv.c0 = std::cos(dv.w * dv.t0);
+        dv.s1 = std::sin(dv.w * dv.t1);
+        dv.c1 = std::cos(dv.w * dv.t1);
+        dv.axis = prm_.wall_drive_axis;
+        dv.first = tstep_ == 0;
+        launch(k_adj_drive<D>, nb, TPB, 0, st_, S(), n, adj_, dv);
+    }
     launch(k_adj_param_sum<D>, RB, CG_BLOCK, 0, st_, n, adj_, partials_.p, ticket_.p, adjsum_.p);
     MPS_CUDA(cudaGetLastError());
     unsigned e = 0;
@@ -1899,9 +1955,10 @@ int mps_adjoint_seed(mps_session *s, const double *lam_pos, const double *lam_ve
 
 int mps_step_adjoint(mps_session *s) { MPS_API_BODY(s, s->eng->step_adjoint()); }
 
-int mps_adjoint_get(mps_session *s, double *lam_pos, double *lam_vel, double *grad_gravity, double *grad_viscosity)
+int mps_adjoint_get(mps_session *s, double *lam_pos, double *lam_vel, double *grad_gravity, double *grad_viscosity,
+                    double *grad_drive)
 {
-    MPS_API_BODY(s, s->eng->adjoint_get(lam_pos, lam_vel, grad_gravity, grad_viscosity));
+    MPS_API_BODY(s, s->eng->adjoint_get(lam_pos, lam_vel, grad_gravity, grad_viscosity, grad_drive));
 }
 
 }  // extern "C"

@@ -43,6 +43,7 @@ struct Adj {
     double *lp;                // adjoint of P
     double *mu;                // PPE adjoint solution
     double *nv;                // per-particle viscosity gradient terms
+    double *dA, *df;           // per-particle wall-drive gradient terms (amplitude, frequency)
     int *pmi;                  // P_min argument (reference index)
     int *evn, *evj;            // collision impulses per particle, partner of each
     double *evd;               // per impulse: partner velocity adjoint (D), separation adjoint (D)
@@ -329,10 +330,12 @@ __global__ void k_adj_collision(CellSource<D> src, State<D> s, Consts k, int n, 
     if (i >= n) return;
     int q = s.id[i];
     if (s.type[i] != FLUID) {
+        // walls and dummies pass through the collision unchanged (x^c = x*, u^c = u*)
+        bool g = s.type[i] == GHOST;
 #pragma unroll
         for (int d = 0; d < D; d++) {
-            a.lxs[d][q] = 0.0;
-            a.lus[d][q] = 0.0;
+            a.lxs[d][q] = g ? 0.0 : a.lxc[d][q];
+            a.lus[d][q] = g ? 0.0 : a.luc[d][q];
         }
         a.evn[q] = 0;
         return;
@@ -424,15 +427,16 @@ __global__ void k_adj_collision(CellSource<D> src, State<D> s, Consts k, int n, 
     a.evn[q] = nev;
 }
 
-// Partner terms of the impulses: particle p adds what every fluid i that
-// hit it recorded (i is in p's candidate set, which is symmetric).
+// Partner terms of the impulses: particle p (fluid, or a wall or dummy, whose
+// adjoint feeds the wall drive's gradient) adds what every fluid i that hit
+// it recorded (i is in p's candidate set, which is symmetric).
 template <int D>
 __global__ void k_adj_collision_gather(CellSource<D> src, State<D> s, int n, Adj<D> a)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int q = s.id[i];
-    if (s.type[i] != FLUID) return;
+    if (s.type[i] == GHOST) return;
     double lu[D], lx[D];
 #pragma unroll
     for (int d = 0; d < D; d++) lu[d] = lx[d] = 0.0;
@@ -457,14 +461,14 @@ __global__ void k_adj_collision_gather(CellSource<D> src, State<D> s, int n, Adj
     }
 }
 
-// Without collision x^c = x*, u^c = u* (fluid).
+// Without collision x^c = x*, u^c = u*.
 template <int D>
 __global__ void k_adj_no_collision(State<D> s, int n, Adj<D> a)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int q = s.id[i];
-    bool f = s.type[i] == FLUID;
+    bool f = s.type[i] != GHOST;
 #pragma unroll
     for (int d = 0; d < D; d++) {
         a.lxs[d][q] = f ? a.lxc[d][q] : 0.0;
@@ -488,8 +492,10 @@ __global__ void k_adj_accel(State<D> s, Consts k, int n, Adj<D> a)
 // Viscosity (operators.c:50-85) and the explicit update in reverse, gather
 // form, on the previous step's list (state = the step's input):
 //   a_i = g + nu c sum_j (u_j - u_i) w_L(r_ij)   (fluid i)
-// Writes the adjoint of the step's input x, u (fluid only) over a.lx,
-// a.lu, and the per-particle gravity and viscosity gradient terms.
+// Writes the adjoint of the step's input x, u over a.lx, a.lu (walls and
+// dummies: of their prescribed positions and velocities at the step's
+// start, for the wall drive's gradient), and the per-particle gravity and
+// viscosity gradient terms.
 template <int D>
 __global__ void k_adj_viscosity(CellSource<D> src, State<D> s, Consts k, int n, Adj<D> a)
 {
@@ -543,38 +549,81 @@ __global__ void k_adj_viscosity(CellSource<D> src, State<D> s, Consts k, int n, 
             for (int d = 0; d < D; d++) lx[d] -= h * e[d] / r;
         }
     });
+    bool live = s.type[i] != GHOST;
 #pragma unroll
     for (int d = 0; d < D; d++) {
-        a.lx[d][q] = fi ? lx[d] : 0.0;
-        a.lu[d][q] = fi ? lu[d] : 0.0;
+        a.lx[d][q] = live ? lx[d] : 0.0;
+        a.lu[d][q] = live ? lu[d] : 0.0;
         a.gv[d][q] = fi ? lai[d] : 0.0;
     }
     a.nv[q] = fi ? k.coeff * vterm : 0.0;
 }
 
-// Deterministic sums of the per-particle gravity (D) and viscosity terms
-// over [0, n), added to out[0..D].
+// Wall drive x = rest + A sin(w t), u = A w cos(w t), w = 2 pi f, along the
+// drive axis: a wall or dummy particle's adjoints of its prescribed
+// position and velocity at the step's end (t1: lxs, lus) and start (t0:
+// lx, lu) give its terms of dL/dA and dL/df; its step-start adjoints are
+// then cleared (a prescribed state has no earlier dependence).  `first`:
+// the step starts from the uploaded state, whose wall velocity is not the
+// drive's.
+struct DriveT {
+    double A, w, t0, t1, s0, c0, s1, c1;
+    int axis, first;
+};
+
+template <int D>
+__global__ void k_adj_drive(State<D> s, int n, Adj<D> a, DriveT dv)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int q = s.id[i];
+    int t = s.type[i];
+    double gA = 0.0, gf = 0.0;
+    if (t == WALL || t == DUMMY) {
+        const double tp = 2.0 * 3.14159265358979323846;
+        double lx1 = a.lxs[dv.axis][q], lu1 = a.lus[dv.axis][q];
+        double lx0 = a.lx[dv.axis][q], lu0 = dv.first ? 0.0 : a.lu[dv.axis][q];
+        gA = lx1 * dv.s1 + lu1 * dv.w * dv.c1 + lx0 * dv.s0 + lu0 * dv.w * dv.c0;
+        gf = tp * (lx1 * dv.A * dv.c1 * dv.t1 + lu1 * (dv.A * dv.c1 - dv.A * dv.w * dv.s1 * dv.t1) +
+                   lx0 * dv.A * dv.c0 * dv.t0 + lu0 * (dv.A * dv.c0 - dv.A * dv.w * dv.s0 * dv.t0));
+    }
+    a.dA[q] = gA;
+    a.df[q] = gf;
+    if (t != FLUID) {
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+            a.lx[d][q] = 0.0;
+            a.lu[d][q] = 0.0;
+        }
+    }
+}
+
+// Deterministic sums of the per-particle gravity (D), viscosity and wall
+// drive (amplitude, frequency) terms over [0, n), added to out[0..D+2].
 template <int D>
 __global__ void k_adj_param_sum(int n, Adj<D> a, double *partials, unsigned *ticket, double *out)
 {
+    constexpr int NC = D + 3;
     __shared__ double sh[CG_BLOCK / 32];
-    double acc[D + 1];
+    double acc[NC];
 #pragma unroll
-    for (int c = 0; c <= D; c++) acc[c] = 0.0;
+    for (int c = 0; c < NC; c++) acc[c] = 0.0;
     for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
 #pragma unroll
         for (int d = 0; d < D; d++) acc[d] += a.gv[d][q];
         acc[D] += a.nv[q];
+        acc[D + 1] += a.dA[q];
+        acc[D + 2] += a.df[q];
     }
 #pragma unroll
-    for (int c = 0; c <= D; c++) {
+    for (int c = 0; c < NC; c++) {
         double t = block_sum<CG_BLOCK>(acc[c], sh);
-        if (threadIdx.x == 0) partials[(size_t)blockIdx.x * (D + 1) + c] = t;
+        if (threadIdx.x == 0) partials[(size_t)blockIdx.x * NC + c] = t;
     }
     if (last_block(ticket, gridDim.x)) {
 #pragma unroll
-        for (int c = 0; c <= D; c++) {
-            double tot = final_sum(partials, gridDim.x, D + 1, c, sh);
+        for (int c = 0; c < NC; c++) {
+            double tot = final_sum(partials, gridDim.x, NC, c, sh);
             if (threadIdx.x == 0) out[c] += tot;
         }
     }

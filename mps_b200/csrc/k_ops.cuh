@@ -12,6 +12,7 @@
 //   surface flags        operators.c:206-219, 253-267
 //   P_min + gradient     operators.c:102-181
 //   correction, wall, out-of-bounds   simulation.c:100-117, boundary.c:12-61
+//   driven walls                      no counterpart (fixed walls when A = 0)
 #pragma once
 
 #include "device.cuh"
@@ -63,6 +64,32 @@ __global__ void k_explicit_update(State<D> s, Consts k, int n)
         s.vel[d][i] = v;
         s.pos[d][i] = s.pos[d][i] + k.dt * v;
     }
+}
+
+// Driven walls (no counterpart in the reference): every WALL and DUMMY
+// particle at rest + dx along `axis` with velocity vel there, the values of
+// the drive at the end of the step.
+template <int D>
+__global__ void k_drive_walls(State<D> s, int n, const double *__restrict__ rest, int axis, double dx, double vel)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int t = s.type[i];
+    if (t != WALL && t != DUMMY) return;
+    s.pos[axis][i] = rest[s.id[i]] + dx;
+#pragma unroll
+    for (int d = 0; d < D; d++) s.vel[d][i] = 0.0;
+    s.vel[axis][i] = vel;
+}
+
+// Rest position of every particle, rest[d * stride + reference index].
+template <int D>
+__global__ void k_set_rest(State<D> s, int n, int stride, double *__restrict__ rest)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int d = 0; d < D; d++) rest[(size_t)d * stride + s.id[i]] = s.pos[d][i];
 }
 
 // Impulse of partner j on v_i; the same tests and order as the reference.
@@ -280,9 +307,13 @@ __global__ void k_correct(State<D> s, Consts k, int n, int do_correct, int do_wa
             s.pos[d][i] = s.pos[d][i] + k.dt * du;
         }
     }
-    if (do_wall && (t == WALL || t == GHOST)) {
+    if (do_wall && (t == GHOST || (t == WALL && !k.drive_on))) {
 #pragma unroll
         for (int d = 0; d < D; d++) { s.vel[d][i] = 0.0; s.acc[d][i] = 0.0; }
+    }
+    if (do_wall && t == WALL && k.drive_on) {   // driven walls keep their prescribed velocity
+#pragma unroll
+        for (int d = 0; d < D; d++) s.acc[d][i] = 0.0;
     }
     if (do_oob && t == FLUID) {
         bool out = false;

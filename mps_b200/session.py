@@ -181,14 +181,22 @@ class Session:
         self._check(self.lib.mps_step_adjoint(self.h))
 
     def adjoint_get(self):
-        """(lam_pos, lam_vel, grad_gravity, grad_viscosity)."""
+        """(lam_pos, lam_vel, grad_gravity, grad_viscosity, grad_drive[amp, freq])."""
         lx = np.zeros((self.n, self.dim), dtype=np.float64)
         lu = np.zeros((self.n, self.dim), dtype=np.float64)
         gg = np.zeros(self.dim, dtype=np.float64)
+        gd = np.zeros(2, dtype=np.float64)
         gn = C.c_double()
         self._check(self.lib.mps_adjoint_get(self.h, lx.ctypes.data, lu.ctypes.data, gg.ctypes.data,
-                                             C.byref(gn)))
-        return lx, lu, gg, gn.value
+                                             C.byref(gn), gd.ctypes.data))
+        return lx, lu, gg, gn.value, gd
+
+    def set_wall_drive(self, amp: float, freq: float, axis: int = 0):
+        """Driven walls (mps_params_t.wall_drive_*); amp = 0 is the reference's fixed walls."""
+        self.params.wall_drive_amp = float(amp)
+        self.params.wall_drive_freq = float(freq)
+        self.params.wall_drive_axis = int(axis)
+        self._check(self.lib.mps_update_params(self.h, C.byref(self.params)))
 
 
 def start(cfg, dim: int, hp: HostParticles, capacity: int | None = None, **kw) -> Session:

@@ -141,6 +141,9 @@ class Workload:
     types: np.ndarray
     params: dict = field(default_factory=dict)
     steps: int = 1
+    # driven walls (amplitude m, frequency Hz, axis); not a reference deck key,
+    # set on the session parameters (mps_params_t.wall_drive_*)
+    drive: tuple = (0.0, 0.0, 0)
 
     @property
     def n(self):
@@ -215,6 +218,18 @@ def dambreak(name: str, seed: int = 0, jitter: float = 0.01, vel_sigma: float = 
         params["gravity_y"] = repr(-9.81 * gravity_scale)
     suffix = "" if l0 == l0d else f"@l0={l0}"
     return Workload(name + suffix, dim, pos, vel, t, params, nsteps)
+
+
+def sloshing3d(l0: float = 0.004, seed: int = 0, jitter: float = 0.01, amp: float = 0.01, freq: float = 1.5,
+               steps: int = 500, dt: float = 4.0e-4, domain=(0.6, 0.4, 0.3), depth: float = 0.2) -> Workload:
+    """3-D sloshing: tank 0.6 x 0.4 x 0.3 m (y vertical) filled to `depth`,
+    walls driven sinusoidally along x (amplitude `amp`, frequency `freq`),
+    the dam break's lattice rules and parameters otherwise."""
+    water = (domain[0], depth, domain[2])
+    pos, t = dambreak3d_lattice(l0, domain, water)
+    pos = jitter_fluid(pos, t, l0, jitter, seed)
+    params = common_params(3, l0, dt, steps, domain)
+    return Workload(f"sloshing3d@l0={l0}", 3, pos, np.zeros_like(pos), t, params, steps, drive=(amp, freq, 0))
 
 
 def small_dambreak3d(l0: float = 0.02, seed: int = 0, jitter: float = 0.01,

@@ -1039,7 +1039,29 @@ void oracle_remove_out_of_bounds(ParticleSystem *ps, const SimConfig *cfg)
 /* One time step (3P simulation.c:19-118; 2D simulation.c:25-118)      */
 /* ------------------------------------------------------------------ */
 
+/* Driven walls (no counterpart in the reference): the phase terms of a wall
+ * drive at time t, evaluated with the expressions the GPU engine uses on its
+ * host, so both produce the same bits. */
+void oracle_wall_drive_terms(double amp, double freq, double t, double *dx, double *vel)
+{
+    double w = 2.0 * 3.14159265358979323846 * freq;
+    double ph = w * t;
+    *dx = amp * sin(ph);
+    *vel = amp * w * cos(ph);
+}
+
 int oracle_step(ParticleSystem *ps, NeighborList *nl, CellList *cl, const SimConfig *cfg)
+{
+    return oracle_step_driven(ps, nl, cl, cfg, NULL, 0.0, 0.0, 0, 0);
+}
+
+/* oracle_step with driven walls: after the explicit update every WALL and
+ * DUMMY particle is put at rest[i] + A sin(2 pi f t1) along `axis` with the
+ * matching velocity (t1 = (step + 1) dt, the time at the end of the step),
+ * and the wall boundary keeps that velocity instead of zeroing it.  amp = 0
+ * is oracle_step. */
+int oracle_step_driven(ParticleSystem *ps, NeighborList *nl, CellList *cl, const SimConfig *cfg,
+                       const double *rest, double amp, double freq, int axis, int step)
 {
     double re = fmax(cfg->influence_radius_lap, cfg->influence_radius_n);
     if (cfg->surface_tension_enabled) return -2;   /* outside the restated path */
@@ -1060,6 +1082,18 @@ int oracle_step(ParticleSystem *ps, NeighborList *nl, CellList *cl, const SimCon
         Particle *p = &ps->particles[i];
         if (p->type != MPS_FLUID) continue;
         for (int d = 0; d < D; d++) p->pos[d] += dt * p->vel[d];
+    }
+    int driven = amp != 0.0 && rest != NULL;
+    if (driven) {
+        double dx, vel;
+        oracle_wall_drive_terms(amp, freq, (double)(step + 1) * dt, &dx, &vel);
+        for (int i = 0; i < n; i++) {
+            Particle *p = &ps->particles[i];
+            if (p->type != MPS_WALL && p->type != MPS_DUMMY) continue;
+            p->pos[axis] = rest[i] + dx;
+            for (int d = 0; d < D; d++) p->vel[d] = 0.0;
+            p->vel[axis] = vel;
+        }
     }
 #if D == 3
     if (cfg->collision_distance_ratio > 0.0)
@@ -1087,7 +1121,17 @@ int oracle_step(ParticleSystem *ps, NeighborList *nl, CellList *cl, const SimCon
             p->pos[d] += dt * du;
         }
     }
-    oracle_apply_wall_boundary(ps);
+    if (driven) {
+        for (int i = 0; i < n; i++) {
+            Particle *p = &ps->particles[i];
+            if (p->type == MPS_GHOST)
+                for (int d = 0; d < D; d++) { p->vel[d] = 0.0; p->acc[d] = 0.0; }
+            else if (p->type == MPS_WALL)
+                for (int d = 0; d < D; d++) p->acc[d] = 0.0;
+        }
+    } else {
+        oracle_apply_wall_boundary(ps);
+    }
     oracle_remove_out_of_bounds(ps, cfg);
     return 0;
 }

@@ -62,6 +62,9 @@ void oracle_remove_out_of_bounds(ParticleSystem *ps, const SimConfig *cfg);
 
 /* Stage hooks of one time step, in the reference's order. */
 int  oracle_step(ParticleSystem *ps, NeighborList *nl, CellList *cl, const SimConfig *cfg);
+int  oracle_step_driven(ParticleSystem *ps, NeighborList *nl, CellList *cl, const SimConfig *cfg,
+                        const double *rest, double amp, double freq, int axis, int step);
+void oracle_wall_drive_terms(double amp, double freq, double t, double *dx, double *vel);
 
 /* Iteration count and final recursive residual of the last PPE solve. */
 int    oracle_last_iterations(void);

@@ -68,6 +68,7 @@ class Oracle:
             "oracle_apply_wall_boundary": (None, [PS]),
             "oracle_remove_out_of_bounds": (None, [PS, CF]),
             "oracle_step": (C.c_int, [PS, NL, CL, CF]),
+            "oracle_step_driven": (C.c_int, [PS, NL, CL, CF, P, C.c_double, C.c_double, C.c_int, C.c_int]),
             "oracle_last_iterations": (C.c_int, []),
             "oracle_last_residual": (C.c_double, []),
         }
@@ -110,6 +111,13 @@ class Oracle:
 
     def step(self, hp, nl, cl, cfg) -> int:
         return self.lib.oracle_step(C.byref(hp.ps), C.byref(nl.nl), C.byref(cl), C.byref(cfg))
+
+    def step_driven(self, hp, nl, cl, cfg, rest: np.ndarray, amp: float, freq: float, axis: int, step: int) -> int:
+        """A step with driven walls (rest: the walls' rest coordinate along
+        `axis`, per particle; step: index of the step being taken)."""
+        rest = np.ascontiguousarray(rest, dtype=np.float64)
+        return self.lib.oracle_step_driven(C.byref(hp.ps), C.byref(nl.nl), C.byref(cl), C.byref(cfg),
+                                           rest.ctypes.data, amp, freq, axis, step)
 
 
 class Reference:

@@ -31,6 +31,7 @@ Source lines followed (reference 3P unless noted):
   PPE                    pressure_solver.c:411-551 (matrix, rhs :328-340)
   P_min and gradient     operators.c:102-181
   correction, boundary   simulation.c:100-117, boundary.c:12-61
+  driven walls           no counterpart (oracle_step_driven; fixed walls at A = 0)
 """
 from __future__ import annotations
 
@@ -143,10 +144,14 @@ def _collision(xs, us, key, types, mprev, c):
     return v
 
 
-def step(x, u, key, types, g, nu, c):
+def step(x, u, key, types, g, nu, c, drive=None):
     """One step.  x, u: (N, dim) FP64 tensors (may require grad); key: the
     positions of the last neighbour search (previous step's list), no grad;
     types: int tensor; g: (dim,) gravity; nu: scalar viscosity.
+    drive: None, or driven walls as dict(amp, freq (tensors), axis, rest
+    (N, dim) positions at t = 0, t1 = time at the end of this step): WALL
+    and DUMMY particles go to rest + amp sin(2 pi freq t1) along axis with
+    the matching velocity after the explicit update, and keep it.
     Returns (x, u, key, types, info) after the step."""
     dim = c["dim"]
     fluid = types == FLUID
@@ -160,6 +165,18 @@ def step(x, u, key, types, g, nu, c):
     a = g[None, :] + (nu * c["coeff"]) * lap
     us = u + c["dt"] * a * fl
     xs = x + c["dt"] * us * fl
+    walls = (types == WALL) | (types == DUMMY)
+    if drive is not None:
+        om = 2.0 * np.pi * drive["freq"]
+        ph = om * drive["t1"]
+        ax = drive["axis"]
+        onehot = torch.zeros(dim, dtype=x.dtype, device=x.device)
+        onehot[ax] = 1.0
+        xw = drive["rest"] + (drive["amp"] * torch.sin(ph)) * onehot[None, :] + \
+            (x - drive["rest"]) * (1.0 - onehot[None, :])
+        uw = (drive["amp"] * om * torch.cos(ph)) * onehot[None, :].expand_as(u)
+        xs = torch.where(walls[:, None], xw, xs)
+        us = torch.where(walls[:, None], uw, us)
     # 2. collision
     if c["col_on"]:
         uc_v = _collision(xs, us, key, types, mprev, c)
@@ -208,6 +225,8 @@ def step(x, u, key, types, g, nu, c):
         out = fluid & (torch.any((xn < lo) | (xn > hi), dim=1) | torch.any(torch.isnan(xn), dim=1))
         ntypes = torch.where(out, torch.full_like(types, GHOST), types)
     still = (ntypes == FLUID)[:, None]
+    if drive is not None:
+        still = still | walls[:, None]
     un = torch.where(still, un, torch.zeros_like(un))
     info = dict(P=P, n=n, surf=surf, unknown=unk)
     return xn, un, xc.detach(), ntypes, info

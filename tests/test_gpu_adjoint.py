@@ -63,7 +63,7 @@ def _gpu_grad(wl, steps, every=1, precision=_lib.PREC_FP64, gscale=1.0):
     cx, cu = _weights(wl.n, wl.dim)
     fl = (t == 0)[:, None]
     loss = float(np.sum(cx * x * fl) + np.sum(cu * u * fl))
-    dx0, du0, dgs, dnu = roll.backward(cx * fl, cu * fl)
+    dx0, du0, dgs, dnu, _, _ = roll.backward(cx * fl, cu * fl)
     out = dict(loss=loss, dx0=dx0, du0=du0, dgs=dgs, dnu=dnu, n0=roll.n0, lam=roll.lam, types=t, x=x)
     roll.close()
     return out
@@ -152,7 +152,7 @@ def test_adjoint_matches_central_differences():
 
     base, t0 = loss(wl.vel, 1.0, nu0)
     fl = (t0 == 0)[:, None]
-    _, du0, dgs, dnu = roll.backward(cx * fl, cu * fl)
+    _, du0, dgs, dnu, _, _ = roll.backward(cx * fl, cu * fl)
     h = 1e-6
     lp, tp = loss(wl.vel, 1.0 + h, nu0)
     lm, tm = loss(wl.vel, 1.0 - h, nu0)
@@ -212,8 +212,119 @@ def test_torch_autograd_function():
     loss.backward()
     lam = (2.0 * (x.detach() - target) / int(fl.sum())) * fl
     roll.forward(wl.vel, 1.0, roll.cfg.viscosity)
-    _, du0, dgs, dnu = roll.backward(lam.numpy(), np.zeros_like(wl.vel))
+    _, du0, dgs, dnu, _, _ = roll.backward(lam.numpy(), np.zeros_like(wl.vel))
     assert np.allclose(u0.grad.numpy(), du0, rtol=0, atol=1e-14 * max(1.0, np.abs(du0).max()))
     assert float(gs.grad) == pytest.approx(dgs, rel=1e-13)
     assert float(nu.grad) == pytest.approx(dnu, rel=1e-13)
+    roll.close()
+
+
+# ---- driven walls ---------------------------------------------------------------
+
+def _slosh(seed=21):
+    wl = W.sloshing3d(l0=0.02, seed=seed, amp=0.01, freq=5.0, domain=(0.2, 0.15, 0.1), depth=0.08)
+    rng = np.random.default_rng(seed)
+    f = wl.types == 0
+    wl.vel[f] = rng.normal(0.0, 0.05, size=(int(f.sum()), 3))
+    return wl
+
+
+def test_driven_walls_forward_matches_oracle():
+    """Three driven steps against oracle_step_driven: wall positions and
+    velocities bit for bit, neighbour-dependent results within the PPE
+    tolerances of the undriven parity tests; amplitude 0 is the undriven step."""
+    _cuda()
+    from mps_b200 import config as CF
+    from mps_b200 import types as T
+    from mps_b200.session import start
+    from oracle.pyoracle import Oracle
+    wl = _slosh()
+    amp, freq, axis = wl.drive
+    cfg = wl.config()
+    orc = Oracle(3)
+    hr = T.HostParticles(3, wl.pos, wl.vel, wl.types)
+    orc.initial_params(hr, cfg)
+    re = CF.neighbor_radius(cfg)
+    nl = T.HostNeighborList(hr.n, cfg.max_neighbors)
+    cl = orc.cell_list(hr.n, re, cfg)
+    assert orc.search(nl, hr, cl, re) == 0
+    rest = np.ascontiguousarray(wl.pos[:, axis])
+    hm = T.HostParticles(3, wl.pos, wl.vel, wl.types)
+    s = start(cfg, 3, hm)
+    s.set_wall_drive(amp, freq, axis)
+    for k in range(3):
+        assert orc.step_driven(hr, nl, cl, cfg, rest, amp, freq, axis, k) == 0
+        s.step(1)
+    g, v = s.download(), hr.view
+    w = (wl.types == 1) | (wl.types == 3)
+    assert np.array_equal(g["pos"][w], v["pos"][w]) and np.array_equal(g["vel"][w], v["vel"][w])
+    assert np.array_equal(g["type"], v["type"])
+    assert _rel(g["pressure"], v["pressure"]) < 1e-8
+    assert _rel(g["pos"], v["pos"]) < 1e-13
+    s.close()
+    # amplitude 0: the reference's fixed walls, bit for bit
+    a = start(cfg, 3, T.HostParticles(3, wl.pos, wl.vel, wl.types))
+    b = start(cfg, 3, T.HostParticles(3, wl.pos, wl.vel, wl.types))
+    b.set_wall_drive(0.0, freq, axis)
+    a.step(3)
+    b.step(3)
+    ga, gb = a.download(), b.download()
+    for f in ("pos", "vel", "pressure"):
+        assert np.array_equal(ga[f], gb[f]), f
+    a.close()
+    b.close()
+
+
+def _torch_drive_grad(wl, steps, n0, lam):
+    from oracle import torch_step as TS
+    cfg = wl.config()
+    amp0, freq0, axis = wl.drive
+    c = TS.consts(cfg, 3, n0, lam)
+    u0 = torch.tensor(wl.vel, dtype=torch.float64, requires_grad=True)
+    A = torch.tensor(amp0, dtype=torch.float64, requires_grad=True)
+    F = torch.tensor(freq0, dtype=torch.float64, requires_grad=True)
+    g = torch.tensor([cfg.gravity[d] for d in range(3)], dtype=torch.float64)
+    nu = torch.tensor(cfg.viscosity, dtype=torch.float64)
+    x = torch.tensor(wl.pos, dtype=torch.float64)
+    rest = x.clone()
+    u, key, ty = u0, x.clone(), torch.tensor(wl.types, dtype=torch.int64)
+    for k in range(steps):
+        drv = dict(amp=A, freq=F, axis=axis, rest=rest, t1=float(k + 1) * cfg.dt)
+        x, u, key, ty, _ = TS.step(x, u, key, ty, g, nu, c, drive=drv)
+    cx, cu = _weights(wl.n, 3)
+    fl = (ty == 0)[:, None].to(torch.float64)
+    loss = torch.sum(torch.tensor(cx) * x * fl) + torch.sum(torch.tensor(cu) * u * fl)
+    du0, dA, dF = torch.autograd.grad(loss, (u0, A, F))
+    return du0.numpy(), float(dA), float(dF)
+
+
+def test_adjoint_drive_gradient():
+    """Gradients with respect to the drive's amplitude and frequency and the
+    initial velocities: against the dense FP64 autograd (1e-6) and central
+    differences of the GPU forward (h = 1e-6, 2e-4)."""
+    _cuda()
+    from mps_b200.adjoint import Rollout
+    wl = _slosh(seed=22)
+    amp, freq, axis = wl.drive
+    steps = 4
+    roll = Rollout(wl.config(), 3, wl.pos, wl.types, steps, every=2, drive_axis=axis)
+    cx, cu = _weights(wl.n, 3)
+
+    def loss(a, f):
+        x, u, t = roll.forward(wl.vel, 1.0, roll.cfg.viscosity, a, f)
+        fl = (t == 0)[:, None]
+        return float(np.sum(cx * x * fl) + np.sum(cu * u * fl)), fl
+
+    _, fl = loss(amp, freq)
+    _, du0, _, _, dA, dF = roll.backward(cx * fl, cu * fl)
+    tdu0, tdA, tdF = _torch_drive_grad(wl, steps, roll.n0, roll.lam)
+    f = wl.types == 0
+    assert _rel(du0[f], tdu0[f]) < GRAD_TOL
+    assert abs(dA - tdA) <= GRAD_TOL * abs(tdA)
+    assert abs(dF - tdF) <= GRAD_TOL * abs(tdF)
+    h = 1e-6
+    fd = (loss(amp + h, freq)[0] - loss(amp - h, freq)[0]) / (2 * h)
+    assert abs(fd - dA) <= FD_TOL * abs(dA)
+    fd = (loss(amp, freq + h)[0] - loss(amp, freq - h)[0]) / (2 * h)
+    assert abs(fd - dF) <= FD_TOL * abs(dF)
     roll.close()

@@ -104,3 +104,54 @@ def test_torch_step_gradient_matches_central_differences():
             um[q, 1] -= h
             fd = (loss(up, gs, nu) - loss(um, gs, nu)) / (2 * h)
             assert abs(float(fd) - float(du0[q, 1])) <= 1e-5 * float(torch.max(torch.abs(du0))) + 1e-10
+
+
+def test_torch_step_driven_matches_oracle():
+    """Driven walls: three steps against oracle_step_driven (1e-12), and the
+    drive gradients against central differences (h = 1e-6)."""
+    from oracle import torch_step as TS
+    from oracle.pyoracle import Oracle
+    wl = W.sloshing3d(l0=0.02, seed=21, amp=0.01, freq=5.0, domain=(0.2, 0.15, 0.1), depth=0.08)
+    amp, freq, axis = wl.drive
+    cfg = wl.config()
+    orc = Oracle(3)
+    hp = T.HostParticles(3, wl.pos, wl.vel, wl.types)
+    orc.initial_params(hp, cfg)
+    c = TS.consts(cfg, 3, hp.ps.n0, hp.ps.lambda_)
+    re = CF.neighbor_radius(cfg)
+    nl = T.HostNeighborList(hp.n, cfg.max_neighbors)
+    cl = orc.cell_list(hp.n, re, cfg)
+    assert orc.search(nl, hp, cl, re) == 0
+    rest_np = np.ascontiguousarray(wl.pos[:, axis])
+    g = torch.tensor([cfg.gravity[d] for d in range(3)], dtype=torch.float64)
+    nu = torch.tensor(cfg.viscosity, dtype=torch.float64)
+
+    def run(A, F, oracle=False):
+        x = torch.tensor(wl.pos, dtype=torch.float64)
+        rest = x.clone()
+        u, key, ty = torch.tensor(wl.vel, dtype=torch.float64), x.clone(), torch.tensor(wl.types, dtype=torch.int64)
+        for k in range(3):
+            drv = dict(amp=A, freq=F, axis=axis, rest=rest, t1=float(k + 1) * cfg.dt)
+            x, u, key, ty, info = TS.step(x, u, key, ty, g, nu, c, drive=drv)
+            if oracle:
+                assert orc.step_driven(hp, nl, cl, cfg, rest_np, amp, freq, axis, k) == 0
+                v = hp.view
+                assert np.array_equal(ty.numpy(), v["type"])
+                assert _rel(info["P"].numpy(), v["pressure"]) < 1e-12
+                assert _rel(x.numpy(), v["pos"]) < 1e-12
+                assert _rel(u.numpy(), v["vel"]) < 1e-12
+        return x
+
+    run(torch.tensor(amp, dtype=torch.float64), torch.tensor(freq, dtype=torch.float64), oracle=True)
+    rng = np.random.default_rng(3)
+    cx = torch.tensor(rng.normal(size=(wl.n, 3)))
+    A = torch.tensor(amp, dtype=torch.float64, requires_grad=True)
+    F = torch.tensor(freq, dtype=torch.float64, requires_grad=True)
+    dA, dF = torch.autograd.grad(torch.sum(cx * run(A, F)), (A, F))
+    h = 1e-6
+    with torch.no_grad():
+        a, f = torch.tensor(amp, dtype=torch.float64), torch.tensor(freq, dtype=torch.float64)
+        fd = (torch.sum(cx * run(a + h, f)) - torch.sum(cx * run(a - h, f))) / (2 * h)
+        assert abs(float(fd) - float(dA)) <= 1e-5 * abs(float(dA))
+        fd = (torch.sum(cx * run(a, f + h)) - torch.sum(cx * run(a, f - h))) / (2 * h)
+        assert abs(float(fd) - float(dF)) <= 1e-5 * abs(float(dF))
