@@ -1508,13 +1508,14 @@ void Engine<D>::step_adjoint()
         MPS_CUDA(cudaStreamSynchronize(st_));
         double bnorm = std::sqrt(sc_host_->rr_outer);
         if (bnorm > 0.0) {
+            launch(k_adj_scale, RB, CG_BLOCK, 0, st_, n_eq, b_.p, 1.0 / bnorm);
             bool icc = prm_.solver_type == 1;
             PcgBufs<double> v{A_.p,      xf_lo_.p, xf_up_.p, pk_val_lo_.p, pk_val_up_.p, dinv_.p, inv_cm_.p,
                               inv_rm_.p, x_.p,     r_.p,     z_.p,         p_.p,         Ap_.p,   y_.p,
                               part_.p,   b_.p};
-            pcg_solve<double>(v, kAdjRtol * bnorm, prm_.cg_max_iter, icc, n_eq, nnz_);
+            pcg_solve<double>(v, kAdjRtol, prm_.cg_max_iter, icc, n_eq, nnz_);
             launch(k_adj_mu, RB, CG_BLOCK, 0, st_, n_eq, (const int *)part_of_row_.p, (const int *)S().id,
-                   (const double *)x_.p, adj_.mu);
+                   (const double *)x_.p, bnorm, adj_.mu);
         }
     }
     launch(k_adj_ppe_pairs<D>, nb, TPB, 0, st_, cells(), S(), k_, n, adj_, (const int *)row_of_.p);

@@ -233,11 +233,20 @@ __global__ void k_adj_rhs(int n_eq, const int *__restrict__ part_of_row, const i
     }
 }
 
+// b /= ||b||: the adjoint solve runs on a unit right-hand side, so that the
+// CG's absolute breakdown guards (|p.Ap| < 1e-30, |r.z| < 1e-60, kept from
+// pressure_solver.c:294-309 for the forward solve's parity) cannot stop it
+// early when the loss is small.
+__global__ void k_adj_scale(int n_eq, double *__restrict__ b, double s)
+{
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_eq; e += gridDim.x * blockDim.x) b[e] *= s;
+}
+
 __global__ void k_adj_mu(int n_eq, const int *__restrict__ part_of_row, const int *__restrict__ id,
-                         const double *__restrict__ x, double *__restrict__ mu)
+                         const double *__restrict__ x, double scale, double *__restrict__ mu)
 {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n_eq; e += gridDim.x * blockDim.x)
-        mu[id[part_of_row[e]]] = x[e];
+        mu[id[part_of_row[e]]] = x[e] * scale;
 }
 
 // PPE matrix and right-hand side (pressure_solver.c:411-551, rhs :328-340)
