@@ -193,6 +193,22 @@ def ncu_traffic(kernel: str):
 # the B200 arm
 # ---------------------------------------------------------------------------
 
+def max_over_ranks(x: float, dist, device) -> float:
+    """The job's time: the maximum of a per-rank time over all ranks (one
+    independent replica per rank, so the job ends with its slowest rank)."""
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_value(n_fluid_per_rank: int, world: int, steps: int, seconds: float) -> float:
+    """Fluid particle-steps per second of all replicas together."""
+    return n_fluid_per_rank * world * steps / seconds
+
+
 def run_b200(args, rank: int, world: int, local_rank: int):
     import numpy as np
     import torch
@@ -257,13 +273,8 @@ def run_b200(args, rank: int, world: int, local_rank: int):
     pmet = sess.metrics()
     sess.set_profiling(False)
 
-    # max over ranks of the timed region
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    fluid_total = wl.n_fluid * world
-    value = fluid_total * args.steps / (ms_max / 1e3)
+    ms_max = max_over_ranks(ms, dist, "cuda")
+    value = whole_job_value(wl.n_fluid, world, args.steps, ms_max / 1e3)
     iters = met["total_iterations"]
 
     sess.close()
@@ -457,7 +468,12 @@ def run_e2e(wl, cfg, args, torch, dist):
     torch.cuda.synchronize()
     if dist is not None:
         dist.barrier()
-    t0 = time.perf_counter()
+    # the drop-in calls are synchronous (host copies in and out), so CUDA
+    # events on the idle current stream, after a device synchronize, bracket
+    # exactly the loop
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
     for k in range(steps):
         mc_in = int(cnt.max())
         lib.simulation_step(C.byref(ps), C.byref(nl), cl, 2 + k)
@@ -466,17 +482,17 @@ def run_e2e(wl, cfg, args, torch, dist):
         # the used columns of the list (pitched copy), the cell chains back
         h2d += n * dt_p.itemsize + 4 * n + 4 * n * mc_in
         d2h += n * dt_p.itemsize + 4 * n + 4 * n * mc_out + 4 * cl.contents.total_cells + 4 * n
-    wall = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    ev1.record()
+    torch.cuda.synchronize()
+    wall = ev0.elapsed_time(ev1) / 1e3
     ok = lib.mps_dropin_last_status() == 0
     lib.mps_dropin_release(C.byref(ps))
-    t = torch.tensor([wall], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    wall = float(t.item())
+    wall = max_over_ranks(wall, dist, "cuda")
     if not ok:
         return None
     world = dist.get_world_size() if dist is not None else 1
-    return {"value": wl.n_fluid * world * steps / wall, "unit": UNIT,
+    return {"value": whole_job_value(wl.n_fluid, world, steps, wall), "unit": UNIT,
             "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
             "ms_per_step": wall / steps * 1e3,
             "call": "simulation_step(ps, nl, cl, step) of libmps3d.so, pinned host AoS + NeighborList"}
