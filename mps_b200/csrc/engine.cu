@@ -224,6 +224,7 @@ private:
     DevArray<unsigned char> pk_k_lo_, pk_k_up_;
     DevArray<int2> adesc_;
     DevArray<int> xlen_lo_, xlen_up_, xp_lo_, xp_up_, xc_lo_, xc_up_;   // packed cross-cell runs (CSR)
+    DevArray<int> xs_lo_, xs_up_;                                        // head/tail split of each run
     DevArray<double> xf_lo_, xf_up_;
     DevArray<int> inv_len_, inv_off_;        // in-cell block inverses: entries, offsets per active cell
     DevArray<double> inv_cm_, inv_rm_;       // column-major (forward) and row-major (backward) copies
@@ -243,11 +244,10 @@ private:
     int nx_lo_ = 0, nx_up_ = 0;   // entries of the packed cross-cell runs
     int ninv_ = 0;            // entries of the in-cell block inverses
     int spmv_lpr_ = 8;   // lanes per row of the CG SpMV (MPS_SPMV_LPR: 8, 16 or 32)
-    int cross_lpr_ = 8;  // lanes per row of the sweeps' cross-cell products (MPS_CROSS_LPR: 4, 8, 16)
-    // CG-loop kernels launched as programmatic dependents (MPS_PDL_MASK): 1 the
-    // cross-cell sweep kernel, 2 the in-cell sweep kernel, 4 SpMV and vector kernels
+    // CG-loop kernels launched as programmatic dependents (MPS_PDL_MASK): 2 the
+    // colour sweep kernel, 4 SpMV and vector kernels
     int pdl_mask_ = 6;
-    int cell_win_ = CELL_WIN;   // entries per window of the staged in-cell sweep (MPS_CELL_WIN: 1024..4096)
+    int cell_win_ = CELL_WIN;   // entries per window of the staged in-cell sweep (MPS_CELL_WIN: 256..4096)
     bool ppe_valid_ = false;
 
     // ---- driven walls
@@ -336,11 +336,7 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
     if (const char *e = std::getenv("MPS_PDL_MASK")) pdl_mask_ = std::atoi(e) & 7;
     if (const char *e = std::getenv("MPS_CELL_WIN")) {
         int v = std::atoi(e);
-        if (v >= 1024 && v <= CELL_WIN_MAX && v % 4 == 0) cell_win_ = v;
-    }
-    if (const char *e = std::getenv("MPS_CROSS_LPR")) {
-        int v = std::atoi(e);
-        if (v == 4 || v == 8 || v == 16) cross_lpr_ = v;
+        if (v >= 256 && v <= CELL_WIN_MAX && v % 4 == 0) cell_win_ = v;
     }
 
     MPS_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
@@ -349,9 +345,9 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
     MPS_CUDA(cudaMallocHost((void **)&sc_host_, sizeof(CGScalars)));
     MPS_CUDA(cudaMallocHost((void **)&int_host_, 64 * sizeof(int)));
     // the staged in-cell sweeps take more than the default 48 KB of dynamic shared memory
-    MPS_CUDA(cudaFuncSetAttribute(k_sweep_cell<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    MPS_CUDA(cudaFuncSetAttribute(k_sweep_colour<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(sizeof(double) * CELL_STAGE_MAX)));
-    MPS_CUDA(cudaFuncSetAttribute(k_sweep_cell<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    MPS_CUDA(cudaFuncSetAttribute(k_sweep_colour<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(sizeof(double) * CELL_STAGE_MAX)));
     alloc_state();
     build_grid();
@@ -1024,7 +1020,7 @@ void Engine<D>::ppe(bool clamp)
                (const int *)s.cell, (const int *)cell_row0_.p, (const int *)pk_off_lo_.p,
                (const int *)pk_off_up_.p, pk_val_lo_.p, pk_k_lo_.p, pk_val_up_.p, pk_k_up_.p, dinv_.p, err_.p);
         // packed cross-cell runs of the factor for the sweeps
-        for (auto *v : {&xlen_lo_, &xlen_up_, &xp_lo_, &xp_up_}) v->reserve((size_t)n_eq + 1);
+        for (auto *v : {&xlen_lo_, &xlen_up_, &xp_lo_, &xp_up_, &xs_lo_, &xs_up_}) v->reserve((size_t)n_eq + 1);
         launch(k_cross_lengths, nblk(n_eq, TPB), TPB, 0, st_, n_eq, (const int *)row_ptr_.p, (const int *)inpos_.p,
                (const int *)outpos_.p, xlen_lo_.p, xlen_up_.p);
         scan_exclusive<int>(xlen_lo_.p, xp_lo_.p, n_eq, scanws_.p, st_);
@@ -1035,9 +1031,22 @@ void Engine<D>::ppe(bool clamp)
         xf_lo_.reserve((size_t)nx_lo_ + 1);
         xc_up_.reserve((size_t)nx_up_ + 1);
         xf_up_.reserve((size_t)nx_up_ + 1);
+        SweepColours swc{};
+        swc.ncol = ncol;
+        for (int c = 0; c <= ncol; c++) swc.row_off[c] = row_off_[c];
+        for (int k = 0; k < ncol; k++) {
+            // the colour swept just before k, forward (largest non-empty below) and backward
+            int pf = -1, pb = -1;
+            for (int j = k - 1; j >= 0 && pf < 0; j--)
+                if (row_off_[j + 1] > row_off_[j]) pf = j;
+            for (int j = k + 1; j < ncol && pb < 0; j++)
+                if (row_off_[j + 1] > row_off_[j]) pb = j;
+            swc.thr_lo[k] = pf >= 0 ? row_off_[pf] : 0;
+            swc.thr_up[k] = pb >= 0 ? row_off_[pb + 1] : 0x7fffffff;
+        }
         launch(k_cross_fill, nblk(n_eq, TPB), TPB, 0, st_, n_eq, (const int *)row_ptr_.p, (const int *)inpos_.p,
                (const int *)outpos_.p, (const int *)col_.p, (const double *)F_.p, (const int *)xp_lo_.p,
-               (const int *)xp_up_.p, xc_lo_.p, xf_lo_.p, xc_up_.p, xf_up_.p);
+               (const int *)xp_up_.p, xc_lo_.p, xf_lo_.p, xc_up_.p, xf_up_.p, swc, xs_lo_.p, xs_up_.p);
         int nact = act_off_[ncol];
         adesc_.reserve((size_t)nact + 1);
         if (nact)
@@ -1137,22 +1146,22 @@ void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, 
         const int *pko = fwdir ? pk_off_lo_.p : pk_off_up_.p, *pkl = fwdir ? pk_len_lo_.p : pk_len_up_.p;
         const T *pkv = fwdir ? v.pkv_lo : v.pkv_up;
         const unsigned char *pkk = fwdir ? pk_k_lo_.p : pk_k_up_.p;
+        int order[8], nc = 0;
         for (int i = 0; i < ncol; i++) {
             int c = fwdir ? i : ncol - 1 - i;
-            int kb = act_off_[c], ke = act_off_[c + 1];
-            int rb = row_off_[c], re = row_off_[c + 1];
-            if (ke <= kb) continue;
-            auto crossk = k_sweep_cross<8, T>;
-            if (cross_lpr_ == 4) crossk = k_sweep_cross<4, T>;
-            if (cross_lpr_ == 16) crossk = k_sweep_cross<16, T>;
-            lk(1, crossk, nblk((long long)(re - rb) * cross_lpr_, 256), 256, 0, rb, re,
-               (const int *)(fwdir ? xp_lo_.p : xp_up_.p), (const int *)(fwdir ? xc_lo_.p : xc_up_.p),
-               fwdir ? v.xf_lo : v.xf_up, rhs, (const T *)out, v.part, (const CGScalars *)sc_.p);
-            auto cellk = fwdir ? k_sweep_cell<true, T> : k_sweep_cell<false, T>;
-            lk(2, cellk, nwin_[c], CELL_THREADS, sizeof(T) * (cell_win_ + CELL_MAXBLK),
-               (const int *)wfirst_.p + win_off_[c],
-               (const int2 *)adesc_.p, (const int *)inv_off_.p, fwdir ? v.inv_cm : v.inv_rm, pko, pkl, pkv, pkk,
-               v.dinv, (const T *)v.part, out, (const CGScalars *)sc_.p, cell_win_ + CELL_MAXBLK, err_.p);
+            if (act_off_[c + 1] > act_off_[c]) order[nc++] = c;
+        }
+        auto colk = fwdir ? k_sweep_colour<true, T> : k_sweep_colour<false, T>;
+        for (int i = 0; i < nc; i++) {
+            int c = order[i], cn = i + 1 < nc ? order[i + 1] : -1;
+            int nrb = cn >= 0 ? row_off_[cn] : 0, nre = cn >= 0 ? row_off_[cn + 1] : 0;
+            int ncb = cn >= 0 ? nblk((long long)(nre - nrb) * 8, CELL_THREADS) : 0;
+            lk(2, colk, nwin_[c] + ncb, CELL_THREADS, sizeof(T) * (cell_win_ + CELL_MAXBLK),
+               (const int *)wfirst_.p + win_off_[c], nwin_[c], (const int2 *)adesc_.p, (const int *)inv_off_.p,
+               fwdir ? v.inv_cm : v.inv_rm, pko, pkl, pkv, pkk, v.dinv, (const int *)(fwdir ? xp_lo_.p : xp_up_.p),
+               (const int *)(fwdir ? xs_lo_.p : xs_up_.p), (const int *)(fwdir ? xc_lo_.p : xc_up_.p),
+               fwdir ? v.xf_lo : v.xf_up, (int)(i == 0), nrb, nre, rhs, v.part, out, (const CGScalars *)sc_.p,
+               cell_win_ + CELL_MAXBLK, err_.p);
         }
     };
     auto spmv = [&]() {

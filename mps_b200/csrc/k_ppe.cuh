@@ -394,17 +394,16 @@ k_ic0_incell(int kbeg, int kend, const int *__restrict__ acells, const int *__re
 // cross-cell (col >= r0 + m).  `inpos[r]` is the first in-cell position and
 // `outpos[r]` the first upper cross-cell position of row r.
 //
-// A sweep over one colour runs in two kernels:
-//   1. k_sweep_cross: the cross-cell products of every row of the colour,
-//      which depend only on finished colours, LPR lanes per row, into part;
-//   2. k_sweep_cell: the in-cell triangular solve, a warp per cell, as the
-//      product with the inverse of the cell's diagonal block of the factor
-//      (formed once per step after the factorisation, k_cell_inverse): the
-//      same preconditioner as substitution, rounded differently, with no
-//      serial chain through the cell's rows.
-// Cells with more than SWEEP_MAXM unknowns (over twice the most a cell of
-// side re holds at rest spacing; only in a blow-up) are solved row by row by
-// substitution from the packed in-cell runs.
+// A colour's part of a sweep is its cross-cell products (which depend only
+// on finished colours) followed by its in-cell triangular solve.  The solve
+// is the product with the inverse of the cell's diagonal block of the factor
+// (formed once per step after the factorisation, k_cell_inverse): the same
+// preconditioner as substitution, rounded differently, with no serial chain
+// through the cell's rows.  Cells with more than SWEEP_MAXM unknowns (over
+// twice the most a cell of side re holds at rest spacing; only in a blow-up)
+// are solved row by row by substitution from the packed in-cell runs.  One
+// launch per colour (k_sweep_colour) does the colour's in-cell part and the
+// next colour's cross products from colours already finished.
 
 constexpr int SWEEP_MAXM = 64;
 
@@ -428,16 +427,7 @@ __global__ void k_row_splits(int n_eq, const int *__restrict__ row_ptr, const in
     outpos[r] = q;
 }
 
-// ---- split sweeps: cross-cell products, then the in-cell solve -------------
-//
-// k_sweep_cross: every row of a colour (rows [rbeg, rend) are contiguous)
-// sums its cross-cell run against the finished colours, LPR lanes per row,
-// into part[r] = rhs[r] - sum, from the packed cross-run CSR.
-//
-// Both sweep kernels are launched as programmatic dependents (launch_pdl):
-// what they load before pdl_wait() -- row bounds, factor values and columns,
-// block inverses, cell descriptors -- is written once per step, before the
-// CG loop; x, part and the CG scalars are read only after it.
+// ---- packed cross-cell runs ----------------------------------------------------
 
 // Cross-cell runs of the factor, packed once per step into their own CSR
 // (lo: the lower cross run [row_ptr, inpos) of every row, for the forward
@@ -452,63 +442,46 @@ __global__ void k_cross_lengths(int n_eq, const int *__restrict__ row_ptr, const
     len_up[r] = row_ptr[r + 1] - outpos[r];
 }
 
+// Colour bookkeeping of the sweeps: the first row of each colour, and per
+// colour the column thresholds that split a row's packed cross runs by the
+// colour of their entries (rows are numbered colour by colour, so columns
+// are ordered by colour too):
+//   lo run (forward): entries with col >= thr_lo[k] come from the colour
+//     swept just before colour k (its "tail"), the others from earlier ones;
+//   up run (backward): entries with col < thr_up[k] come from the colour
+//     swept just before colour k in the backward order (the tail).
+struct SweepColours {
+    int row_off[9];
+    int thr_lo[8], thr_up[8];
+    int ncol;
+};
+
 __global__ void k_cross_fill(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ inpos,
                              const int *__restrict__ outpos, const int *__restrict__ col,
                              const double *__restrict__ F, const int *__restrict__ xp_lo,
                              const int *__restrict__ xp_up, int *__restrict__ xc_lo, double *__restrict__ xf_lo,
-                             int *__restrict__ xc_up, double *__restrict__ xf_up)
+                             int *__restrict__ xc_up, double *__restrict__ xf_up, SweepColours sc,
+                             int *__restrict__ xs_lo, int *__restrict__ xs_up)
 {
     int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n_eq) return;
-    int o = xp_lo[r];
+    int k = 0;
+    while (k + 1 < sc.ncol && r >= sc.row_off[k + 1]) k++;
+    int o = xp_lo[r], split = o;
     for (int q = row_ptr[r]; q < inpos[r]; q++, o++) {
         xc_lo[o] = col[q];
         xf_lo[o] = F[q];
+        split += col[q] < sc.thr_lo[k];
     }
+    xs_lo[r] = split;
     o = xp_up[r];
+    split = o;
     for (int q = outpos[r]; q < row_ptr[r + 1]; q++, o++) {
         xc_up[o] = col[q];
         xf_up[o] = F[q];
+        split += col[q] < sc.thr_up[k];
     }
-}
-
-// part[r] = rhs[r] - sum over row r's packed cross run of F x, LPR lanes per
-// row, for the rows [rbeg, rend) of one colour.
-template <int LPR, class T>
-__global__ void __launch_bounds__(256)
-k_sweep_cross(int rbeg, int rend, const int *__restrict__ xp, const int *__restrict__ xc, const T *__restrict__ xf,
-              const T *rhs, const T *x, T *part, const CGScalars *sc)
-{
-    constexpr int PF = 4;   // entries per lane loaded before the wait
-    pdl_trigger();
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    int r = rbeg + t / LPR;
-    int lane = t % LPR;
-    int a = 0, b = 0;
-    if (r < rend) {
-        a = __ldg(&xp[r]);
-        b = __ldg(&xp[r + 1]);
-    }
-    T f[PF];
-    int c[PF];
-#pragma unroll
-    for (int u = 0; u < PF; u++) {
-        int q = a + lane + u * LPR;
-        bool ok = q < b;
-        f[u] = ok ? __ldg(&xf[q]) : T(0);
-        c[u] = ok ? __ldg(&xc[q]) : -1;
-    }
-    pdl_wait();
-    if (sc->done) return;
-    T s = T(0);
-#pragma unroll
-    for (int u = 0; u < PF; u++)
-        if (c[u] >= 0) s += f[u] * x[c[u]];
-#pragma unroll 4
-    for (int q = a + lane + PF * LPR; q < b; q += LPR) s += __ldg(&xf[q]) * x[__ldg(&xc[q])];
-#pragma unroll
-    for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LPR);
-    if (lane == 0 && r < rend) part[r] = rhs[r] - s;
+    xs_up[r] = split;
 }
 
 // Packed in-cell factor, built once per step after the factorisation.  For
@@ -680,7 +653,7 @@ constexpr int MBAR_POLLS = 1 << 20;
 // that it overlaps the preceding cross-cell kernel, then its warps take the
 // window's cells in turn.
 
-constexpr int CELL_WIN = 1024;        // default window (entries); MPS_CELL_WIN selects 1024..4096
+constexpr int CELL_WIN = 1024;        // default window (entries); MPS_CELL_WIN selects 256..4096
 constexpr int CELL_WIN_MAX = 4096;
 constexpr int CELL_MAXBLK = ((SWEEP_MAXM * (SWEEP_MAXM + 1) / 2) + 3) & ~3;
 constexpr int CELL_STAGE_MAX = CELL_WIN_MAX + CELL_MAXBLK;
@@ -718,27 +691,78 @@ __global__ void k_gather_colour_offsets(ColourIdx at, int n, const int *__restri
     if (t < n) out[t] = inv_off[at.k[t]];
 }
 
-// In-cell step of one colour: x = L_cc^-1 part (forward) or L_cc^-T part
-// (backward) for every cell of the window, a warp per cell, lane l owning
-// rows l and l + 32; part[r] = rhs[r] - the cross-cell sum.  Cells above
-// SWEEP_MAXM unknowns are solved row by row by substitution from the packed
-// runs.
+// ---- one launch per colour ---------------------------------------------------
+//
+// k_sweep_colour finishes colour c and starts the next colour of the sweep
+// in one launch, with two kinds of CTA:
+//   window CTAs (blockIdx < nwin): for the rows of one window of colour c,
+//     part[r] = base[r] - F x over the row's tail (the entries from the
+//     colour swept just before c, finished by the previous launch), where
+//     base is rhs for the sweep's first colour and otherwise the head sums
+//     left in part by the previous launch; then, after a block barrier, the
+//     in-cell product of every cell of the window from its block inverse,
+//     staged in shared memory by one bulk copy issued before pdl_wait();
+//   cross CTAs: for the rows of the next colour, part[r] = rhs[r] - F x over
+//     the row's head (entries from colours swept before c, all finished).
+// Forward: the lo runs, head [xp, xs), tail [xs, xp+1); backward: the up
+// runs, tail [xp, xs), head [xs, xp+1).  Launched as a programmatic
+// dependent: what it loads before pdl_wait() (row bounds, factor values and
+// columns, block inverses, cell descriptors) is written once per step,
+// before the CG loop; x, part and the CG scalars are read only after it.
 template <bool FWD, class T>
 __global__ void __launch_bounds__(CELL_THREADS, 6)
-k_sweep_cell(const int *__restrict__ wfirst, const int2 *__restrict__ desc, const int *__restrict__ inv_off,
-             const T *__restrict__ inv, const int *__restrict__ pk_off, const int *__restrict__ pk_len,
-             const T *__restrict__ pk_val, const unsigned char *__restrict__ pk_k, const T *__restrict__ dinv,
-             const T *part, T *x, const CGScalars *sc, int stage_elems, unsigned *err)
+k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict__ desc,
+               const int *__restrict__ inv_off, const T *__restrict__ inv, const int *__restrict__ pk_off,
+               const int *__restrict__ pk_len, const T *__restrict__ pk_val, const unsigned char *__restrict__ pk_k,
+               const T *__restrict__ dinv, const int *__restrict__ xp, const int *__restrict__ xs,
+               const int *__restrict__ xc, const T *__restrict__ xf, int first, int nrb, int nre, const T *rhs,
+               T *part, T *x, const CGScalars *sc, int stage_elems, unsigned *err)
 {
+    constexpr int LPR = 8;
     extern __shared__ __align__(128) unsigned char cell_stage[];
     __shared__ __align__(8) unsigned long long bar;
     pdl_trigger();
+    if ((int)blockIdx.x >= nwin) {
+        // cross CTA: head sums of the next colour's rows
+        int t = (blockIdx.x - nwin) * blockDim.x + threadIdx.x;
+        int r = nrb + t / LPR;
+        int lane = t % LPR;
+        int a = 0, b = 0;
+        if (r < nre) {
+            a = FWD ? __ldg(&xp[r]) : __ldg(&xs[r]);
+            b = FWD ? __ldg(&xs[r]) : __ldg(&xp[r + 1]);
+        }
+        T f[4];
+        int cc[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            int q = a + lane + u * LPR;
+            bool ok = q < b;
+            f[u] = ok ? __ldg(&xf[q]) : T(0);
+            cc[u] = ok ? __ldg(&xc[q]) : -1;
+        }
+        pdl_wait();
+        if (sc->done) return;
+        T s = T(0);
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (cc[u] >= 0) s += f[u] * x[cc[u]];
+        for (int q = a + lane + 4 * LPR; q < b; q += LPR) s += __ldg(&xf[q]) * x[__ldg(&xc[q])];
+#pragma unroll
+        for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LPR);
+        if (lane == 0 && r < nre) part[r] = rhs[r] - s;
+        return;
+    }
+    // window CTA
     T *stage = reinterpret_cast<T *>(cell_stage);
     int ka = __ldg(&wfirst[blockIdx.x]), kb = __ldg(&wfirst[blockIdx.x + 1]);
-    int o0 = 0, nel = 0;
+    int o0 = 0, nel = 0, R0 = 0, R1 = 0;
     if (ka < kb) {
         o0 = __ldg(&inv_off[ka]);
         nel = __ldg(&inv_off[kb]) - o0;
+        int2 d0 = __ldg(&desc[ka]), d1 = __ldg(&desc[kb - 1]);
+        R0 = d0.x;
+        R1 = d1.x + d1.y;
     }
     bool staged = nel > 0 && nel <= stage_elems;
     unsigned b = smem_u32(&bar);
@@ -749,31 +773,39 @@ k_sweep_cell(const int *__restrict__ wfirst, const int2 *__restrict__ desc, cons
         mbar_arrive_expect_tx(b, bytes);
         bulk_g2s(smem_u32(stage), inv + o0, bytes, b);
     }
-    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int k = ka + w;
-    int2 dd = make_int2(0, 0);
-    int ok = 0;
-    if (k < kb) {
-        dd = __ldg(&desc[k]);
-        ok = __ldg(&inv_off[k]);
-    }
     pdl_wait();
+    bool done = sc->done;
+    if (!done) {
+        // tails of the window's rows: a few entries each (one neighbouring
+        // colour), so TL lanes per row and CELL_THREADS / TL rows per pass
+        constexpr int TL = 2;
+        int lane = threadIdx.x % TL;
+        for (int base = R0; base < R1; base += CELL_THREADS / TL) {   // block-uniform trip count
+            int r = base + threadIdx.x / TL;
+            T s = T(0);
+            if (r < R1) {
+                int a = FWD ? __ldg(&xs[r]) : __ldg(&xp[r]);
+                int e = FWD ? __ldg(&xp[r + 1]) : __ldg(&xs[r]);
+                for (int q = a + lane; q < e; q += TL) s += __ldg(&xf[q]) * x[__ldg(&xc[q])];
+            }
+            s += __shfl_down_sync(0xffffffffu, s, 1, TL);
+            if (lane == 0 && r < R1) part[r] = (first ? rhs[r] : part[r]) - s;
+        }
+    }
+    __syncthreads();
     if (staged && !mbar_wait(b, 0, MBAR_POLLS)) {
         if (threadIdx.x == 0) atomicOr(err, ERR_COPY_TIMEOUT);
         mbar_wait(b, 0, MBAR_POLLS);
         return;
     }
     if (nel > stage_elems && threadIdx.x == 0) atomicOr(err, ERR_WINDOW_OVERFLOW);
-    if (sc->done) return;
+    if (done) return;
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const T *src = staged ? stage : inv + o0;
-    for (; k < kb; k += CELL_THREADS / 32) {
+    for (int k = ka + w; k < kb; k += CELL_THREADS / 32) {
+        int2 dd = __ldg(&desc[k]);
         int r0 = dd.x, m = dd.y;
-        const T *blk = src + (ok - o0);
-        int kn = k + CELL_THREADS / 32;
-        if (kn < kb) {
-            dd = __ldg(&desc[kn]);
-            ok = __ldg(&inv_off[kn]);
-        }
+        const T *blk = src + (__ldg(&inv_off[k]) - o0);
         if (m > SWEEP_MAXM) {
             for (int t = 0; t < m; t++) {
                 int r = FWD ? r0 + t : r0 + m - 1 - t;
@@ -790,44 +822,43 @@ k_sweep_cell(const int *__restrict__ wfirst, const int2 *__restrict__ desc, cons
         int i0 = lane, i1 = lane + 32;
         T p0 = i0 < m ? part[r0 + i0] : T(0);
         T p1 = i1 < m ? part[r0 + i1] : T(0);
-        // two partial sums per row (even and odd j) halve the dependent add chain
         T a0 = T(0), a1 = T(0), b0 = T(0), b1 = T(0);
         if (m <= 32) {
 #pragma unroll 2
             for (int j = 0; j < m; j += 2) {
-                int k = j + 1;
+                int kk = j + 1;
                 T pj = __shfl_sync(0xffffffffu, p0, j);
-                T pk = __shfl_sync(0xffffffffu, p0, k & 31);
+                T pk = __shfl_sync(0xffffffffu, p0, kk & 31);
                 if (FWD) {
                     if (i0 >= j && i0 < m) a0 += blk[tri_colofs(j, m) + i0 - j] * pj;
-                    if (k < m && i0 >= k && i0 < m) b0 += blk[tri_colofs(k, m) + i0 - k] * pk;
+                    if (kk < m && i0 >= kk && i0 < m) b0 += blk[tri_colofs(kk, m) + i0 - kk] * pk;
                 } else {
                     if (i0 <= j) a0 += blk[j * (j + 1) / 2 + i0] * pj;
-                    if (k < m && i0 <= k) b0 += blk[k * (k + 1) / 2 + i0] * pk;
+                    if (kk < m && i0 <= kk) b0 += blk[kk * (kk + 1) / 2 + i0] * pk;
                 }
             }
         } else {
             for (int j = 0; j < m; j += 2) {
-                int k = j + 1;
+                int kk = j + 1;
                 T pj = __shfl_sync(0xffffffffu, j < 32 ? p0 : p1, j & 31);
-                T pk = __shfl_sync(0xffffffffu, k < 32 ? p0 : p1, k & 31);
+                T pk = __shfl_sync(0xffffffffu, kk < 32 ? p0 : p1, kk & 31);
                 if (FWD) {
                     const T *cj = blk + tri_colofs(j, m) - j;
                     if (i0 >= j) a0 += cj[i0] * pj;
                     if (i1 >= j && i1 < m) a1 += cj[i1] * pj;
-                    if (k < m) {
-                        const T *ck = blk + tri_colofs(k, m) - k;
-                        if (i0 >= k) b0 += ck[i0] * pk;
-                        if (i1 >= k && i1 < m) b1 += ck[i1] * pk;
+                    if (kk < m) {
+                        const T *ck = blk + tri_colofs(kk, m) - kk;
+                        if (i0 >= kk) b0 += ck[i0] * pk;
+                        if (i1 >= kk && i1 < m) b1 += ck[i1] * pk;
                     }
                 } else {
                     const T *rj = blk + j * (j + 1) / 2;
                     if (i0 <= j) a0 += rj[i0] * pj;
                     if (i1 <= j) a1 += rj[i1] * pj;
-                    if (k < m) {
-                        const T *rk = blk + k * (k + 1) / 2;
-                        if (i0 <= k) b0 += rk[i0] * pk;
-                        if (i1 <= k) b1 += rk[i1] * pk;
+                    if (kk < m) {
+                        const T *rk = blk + kk * (kk + 1) / 2;
+                        if (i0 <= kk) b0 += rk[i0] * pk;
+                        if (i1 <= kk) b1 += rk[i1] * pk;
                     }
                 }
             }
