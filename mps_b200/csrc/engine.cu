@@ -995,9 +995,9 @@ void Engine<D>::ppe(bool clamp)
         for (int c = 0; c < ncol; c++) {
             int rb = row_off_[c], re = row_off_[c + 1];
             if (re > rb)
-                launch(k_ic0_cross, nblk(re - rb, 128), 128, 0, st_, rb, re, (const int *)row_ptr_.p,
-                       (const int *)diagpos_.p, (const int *)inpos_.p, (const int *)col_.p, (const double *)A_.p,
-                       F_.p);
+                launch(k_ic0_cross_warp, nblk((long long)(re - rb) * 32, 256), 256, 0, st_, rb, re,
+                       (const int *)row_ptr_.p, (const int *)diagpos_.p, (const int *)inpos_.p, (const int *)col_.p,
+                       (const double *)A_.p, F_.p);
             int kb = act_off_[c], ke = act_off_[c + 1];
             if (ke > kb)
                 launch(k_ic0_incell, nblk(ke - kb, SWEEP_WARPS_IC), 32 * SWEEP_WARPS_IC, 0, st_, kb, ke,

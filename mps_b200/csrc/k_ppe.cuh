@@ -321,17 +321,38 @@ __device__ __forceinline__ void ic0_diag(int r, const int *__restrict__ row_ptr,
     F[pd] = 1.0 / sqrt(d);
 }
 
-// Phase A of a colour: the cross-cell entries of its rows [rbeg, rend),
-// which depend only on finished colours and on earlier entries of the same
-// row.  Thread per row.
-__global__ void k_ic0_cross(int rbeg, int rend, const int *__restrict__ row_ptr, const int *__restrict__ diagpos,
-                            const int *__restrict__ inpos, const int *__restrict__ col,
-                            const double *__restrict__ A, double *F)
+// Phase A, warp per row: the entries of the row stay sequential (each needs
+// the row's earlier entries), but each entry's sparse dot product
+// sum_{j<k} L_rj L_kj is spread over the lanes: they take row k's lower
+// entries j and look each up in the row's finished prefix by binary search,
+// then a warp sum.  This is phase A of a colour: the cross-cell entries of
+// its rows [rbeg, rend), which depend only on finished colours and on
+// earlier entries of the same row.
+__global__ void k_ic0_cross_warp(int rbeg, int rend, const int *__restrict__ row_ptr,
+                                 const int *__restrict__ diagpos, const int *__restrict__ inpos,
+                                 const int *__restrict__ col, const double *__restrict__ A, double *F)
 {
-    int r = rbeg + blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= rend) return;
-    int pin = inpos[r];
-    for (int p = row_ptr[r]; p < pin; p++) ic0_entry(r, p, row_ptr, diagpos, col, A, F);
+    int r = rbeg + (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    int lane = threadIdx.x & 31;
+    if (r >= rend) return;   // warp-uniform
+    int a0 = row_ptr[r], pin = inpos[r];
+    for (int p = a0; p < pin; p++) {
+        int kc = col[p];
+        int b = row_ptr[kc], kd = diagpos[kc];
+        double s = 0.0;
+        for (int q = b + lane; q < kd; q += 32) {
+            int f = find_col(col, a0, p, col[q]);
+            if (f >= 0) s += F[f] * F[q];
+        }
+        s = warp_allsum(s);
+        if (lane == 0) {
+            double lik = (A[p] - s) * F[kd];
+            F[p] = lik;
+            int up = find_col(col, kd + 1, row_ptr[kc + 1], r);
+            if (up >= 0) F[up] = lik;
+        }
+        __syncwarp();
+    }
 }
 
 // Phase B of a colour: in-cell entries and diagonals.  Warp per cell; lane l
