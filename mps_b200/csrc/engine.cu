@@ -267,6 +267,7 @@ private:
     // ---- misc
     DevArray<double> vafter_, pmin_;
     DevArray<int> lptr_, lidx_, lout_, lcnt_;
+    DevArray<int> link_head_, link_next_;   // get_cell_links output, kept across calls
     DevArray<unsigned char> aos_;
     DevArray<double> soa_in_;
     DevArray<int> int_in_;
@@ -831,7 +832,20 @@ void Engine<D>::upload_list(const int *nb, const int *cnt, int max_nb)
     lptr_.reserve((size_t)n + 1);
     MPS_CUDA(cudaMemcpyAsync(lcnt_.p, cnt, sizeof(int) * n, cudaMemcpyHostToDevice, st_));
     scan_exclusive<int>(lcnt_.p, lptr_.p, n, scanws_.p, st_);
-    if (mc > 0 && n > 0) {
+    // a list in page-locked host memory is read in place by the gather
+    // kernel (only the used entries cross the link); a pageable one goes
+    // through a pitched copy of its used columns
+    cudaPointerAttributes pa{};
+    bool mapped = false;
+    if (cudaPointerGetAttributes(&pa, nb) == cudaSuccess)
+        mapped = pa.type == cudaMemoryTypeHost && pa.devicePointer != nullptr;
+    else
+        (void)cudaGetLastError();
+    if (mc > 0 && n > 0 && mapped) {
+        lidx_.reserve((size_t)n * mc);
+        launch(k_gather_host_list, nblk((long long)n * 32, TPB), TPB, 0, st_, (const int *)pa.devicePointer,
+               max_nb, (const int *)lcnt_.p, (const int *)lptr_.p, n, lidx_.p, err_.p);
+    } else if (mc > 0 && n > 0) {
         lout_.reserve((size_t)n * mc);
         lidx_.reserve((size_t)n * mc);
         MPS_CUDA(cudaMemcpy2DAsync(lout_.p, sizeof(int) * mc, nb, sizeof(int) * (size_t)max_nb, sizeof(int) * mc,
@@ -1627,13 +1641,14 @@ void Engine<D>::get_cell_links(int *head, int *next, int total)
     if (!structure_) throw CudaError("no neighbour structure", MPS_ERR_INVALID);
     if (total != g_.total) throw CudaError("cell count differs from the session grid", MPS_ERR_INVALID);
     int n = n_;
-    DevArray<int> h, nx;
-    h.reserve(total + 1);
-    nx.reserve((size_t)n + 1);
+    link_head_.reserve((size_t)total + 1);
+    link_next_.reserve((size_t)n + 1);
     int m = std::max(total, n);
-    if (m) launch(k_cell_links, nblk(m, TPB), TPB, 0, st_, start_.p, S().id, S().cell, total, n, h.p, nx.p);
-    if (head) MPS_CUDA(cudaMemcpyAsync(head, h.p, sizeof(int) * total, cudaMemcpyDeviceToHost, st_));
-    if (next) MPS_CUDA(cudaMemcpyAsync(next, nx.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st_));
+    if (m)
+        launch(k_cell_links, nblk(m, TPB), TPB, 0, st_, start_.p, S().id, S().cell, total, n, link_head_.p,
+               link_next_.p);
+    if (head) MPS_CUDA(cudaMemcpyAsync(head, link_head_.p, sizeof(int) * total, cudaMemcpyDeviceToHost, st_));
+    if (next) MPS_CUDA(cudaMemcpyAsync(next, link_next_.p, sizeof(int) * n, cudaMemcpyDeviceToHost, st_));
     MPS_CUDA(cudaStreamSynchronize(st_));
 }
 

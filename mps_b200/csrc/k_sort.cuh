@@ -152,6 +152,25 @@ __global__ void k_compact_list(const int *__restrict__ rows, int pitch, const in
     }
 }
 
+// The same compaction read straight from a caller's list in page-locked host
+// memory (device-addressable under unified addressing): one warp per row, the
+// lanes striding over the row's count, so only the used entries cross the
+// host link, in 128-byte runs.
+__global__ void k_gather_host_list(const int *__restrict__ rows, int pitch, const int *__restrict__ cnt,
+                                   const int *__restrict__ ptr, int n, int *__restrict__ idx, unsigned *err)
+{
+    long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    int lane = threadIdx.x & 31;
+    if (w >= n) return;
+    int c = min(cnt[w], pitch), o = ptr[w];
+    const int *r = rows + (size_t)w * pitch;
+    for (int k = lane; k < c; k += 32) {
+        int j = r[k];
+        if (j < 0 || j >= n) { atomicOr(err, ERR_LIST_MISMATCH); j = 0; }
+        idx[o + k] = j;
+    }
+}
+
 template <int D>
 __global__ void k_cell_ref_order(const int *__restrict__ cell, const int *__restrict__ id, int n, int *out)
 {

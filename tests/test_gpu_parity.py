@@ -266,6 +266,42 @@ def test_multistep_trajectory_3d():
     assert _rel(g["pos"], o["pos"]) < 1e-12
 
 
+def test_pinned_host_list_matches_pageable_list():
+    """A neighbour list in page-locked host memory (read in place by the
+    gather kernel) drives the same step as the same list in pageable memory
+    (pitched copy), bit for bit; an out-of-range index in it is reported as
+    an error, not followed."""
+    _cuda()
+    import torch
+    from mps_b200 import _lib
+    wl = W.small_dambreak3d(l0=0.02, seed=6)
+    orc = _oracle(3)
+    cfg, hp, nl, cl = _moved_state(wl, orc, steps=1)
+    m = cfg.max_neighbors
+    nb_prev, cnt_prev = nl.neighbors[: hp.n * m].copy(), nl.count[: hp.n].copy()
+    nb_pin = torch.empty(hp.n * m, dtype=torch.int32, pin_memory=True).numpy()
+    cnt_pin = torch.empty(hp.n, dtype=torch.int32, pin_memory=True).numpy()
+    nb_pin[:] = nb_prev
+    cnt_pin[:] = cnt_prev
+    outs = []
+    for nb, cnt in ((nb_prev, cnt_prev), (nb_pin, cnt_pin)):
+        with _session(cfg, 3, hp.copy()) as s:
+            s.set_initial_params(hp.ps.n0, hp.ps.lambda_, hp.ps.n0_count)
+            s.step_with_list(nb, cnt, m)
+            outs.append((s.download(), s.neighbor_list(m)))
+    (ga, (nba, ca)), (gb, (nbb, cb)) = outs
+    for f in ("pos", "vel", "acc", "pressure", "n", "type", "on_surface"):
+        assert np.array_equal(ga[f], gb[f]), f
+    assert np.array_equal(ca, cb)
+    assert np.array_equal(nba, nbb)
+    i = int(np.nonzero(cnt_pin > 0)[0][0])
+    nb_pin[i * m] = hp.n + 5
+    with _session(cfg, 3, hp.copy()) as s:
+        s.set_initial_params(hp.ps.n0, hp.ps.lambda_, hp.ps.n0_count)
+        with pytest.raises(_lib.MpsError):
+            s.step_with_list(nb_pin, cnt_pin, m)
+
+
 def test_neighbor_overflow_reported():
     """max_neighbors too small: an error code, as the reference's exit(1)."""
     _cuda()
