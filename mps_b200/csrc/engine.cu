@@ -247,7 +247,13 @@ private:
     // CG-loop kernels launched as programmatic dependents (MPS_PDL_MASK): 2 the
     // colour sweep kernel, 4 SpMV and vector kernels
     int pdl_mask_ = 6;
-    int cell_win_ = CELL_WIN;   // entries per window of the staged in-cell sweep (MPS_CELL_WIN: 256..4096)
+    // entries per window of the staged in-cell sweep: MPS_CELL_WIN (256..4096)
+    // if set, else 8 KB of inverse entries (1,024 FP64, 2,048 in the mixed
+    // form's FP32 sweeps); win_ is the window of the current tables
+    int cell_win_ = 0;
+    int win_ = CELL_WIN;
+    bool win_valid_ = false;               // the window tables match the current factor and win_
+    std::vector<int> inv_col_off_;         // block-inverse offsets at the colour boundaries
     bool ppe_valid_ = false;
 
     // ---- driven walls
@@ -304,6 +310,7 @@ private:
     void pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, int n_eq, long long nnz,
                    const T *zprev = nullptr);
     void mixed_solve(int n_eq, long long nnz, bool icc);
+    void build_windows(bool fp32);
     static constexpr int kMaxUpdates = 200;      // reliable updates of the mixed form, at most
     static constexpr double kDelta = 0.1;        // FP32 residual reduction between reliable updates
     static constexpr double kAdjRtol = 1.0e-12;  // relative residual of the adjoint PPE solve
@@ -1080,26 +1087,17 @@ void Engine<D>::ppe(bool clamp)
         MPS_CUDA(cudaStreamSynchronize(st_));
         int ninv = int_host_[ncol];
         if (ninv < 0) throw CudaError("in-cell inverses too large for 32-bit offsets", MPS_ERR_UNSUPPORTED);
-        win_off_.assign(ncol + 1, 0);
-        nwin_.assign(ncol, 0);
-        for (int c = 0; c < ncol; c++) {
-            int span = int_host_[c + 1] - int_host_[c];
-            nwin_[c] = act_off_[c + 1] > act_off_[c] ? std::max(1, (span + cell_win_ - 1) / cell_win_) : 0;
-            win_off_[c + 1] = win_off_[c] + nwin_[c] + 1;
-        }
+        inv_col_off_.assign(int_host_, int_host_ + ncol + 1);
         inv_cm_.reserve((size_t)ninv + 1);
         inv_rm_.reserve((size_t)ninv + 1);
-        wfirst_.reserve((size_t)win_off_[ncol] + 1);
         ninv_ = ninv;
         if (nact)
             launch(k_cell_inverse, nblk(nact, 4), 128, 0, st_, nact, (const int2 *)adesc_.p,
                    (const int *)inv_off_.p, (const int *)pk_off_lo_.p, (const int *)pk_len_lo_.p,
                    (const double *)pk_val_lo_.p, (const unsigned char *)pk_k_lo_.p, (const double *)dinv_.p,
                    inv_cm_.p, inv_rm_.p);
-        for (int c = 0; c < ncol; c++)
-            if (nwin_[c])
-                launch(k_inv_windows, nblk(nwin_[c] + 1, TPB), TPB, 0, st_, act_off_[c], act_off_[c + 1],
-                       (const int *)inv_off_.p, cell_win_, nwin_[c], wfirst_.p + win_off_[c]);
+        win_valid_ = false;
+        build_windows(prm_.precision == MPS_PREC_MIXED);
     }
     MPS_CUDA(cudaEventRecord(ev_[3], st_));
 
@@ -1170,12 +1168,12 @@ void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, 
             int c = order[i], cn = i + 1 < nc ? order[i + 1] : -1;
             int nrb = cn >= 0 ? row_off_[cn] : 0, nre = cn >= 0 ? row_off_[cn + 1] : 0;
             int ncb = cn >= 0 ? nblk((long long)(nre - nrb) * 8, CELL_THREADS) : 0;
-            lk(2, colk, nwin_[c] + ncb, CELL_THREADS, sizeof(T) * (cell_win_ + CELL_MAXBLK),
+            lk(2, colk, nwin_[c] + ncb, CELL_THREADS, sizeof(T) * (win_ + CELL_MAXBLK),
                (const int *)wfirst_.p + win_off_[c], nwin_[c], (const int2 *)adesc_.p, (const int *)inv_off_.p,
                fwdir ? v.inv_cm : v.inv_rm, pko, pkl, pkv, pkk, v.dinv, (const int *)(fwdir ? xp_lo_.p : xp_up_.p),
                (const int *)(fwdir ? xs_lo_.p : xs_up_.p), (const int *)(fwdir ? xc_lo_.p : xc_up_.p),
                fwdir ? v.xf_lo : v.xf_up, (int)(i == 0), nrb, nre, rhs, v.part, out, (const CGScalars *)sc_.p,
-               cell_win_ + CELL_MAXBLK, err_.p);
+               win_ + CELL_MAXBLK, err_.p);
         }
     };
     auto spmv = [&]() {
@@ -1243,6 +1241,32 @@ void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, 
         iter_before = sc_host_->iter;
         if (sc_host_->done) break;
     }
+}
+
+// Window tables of the staged in-cell sweeps for the current factor: each
+// colour's range of block inverses split into windows of win_ entries
+// (MPS_CELL_WIN if set, else 8 KB of inverse entries in the precision the
+// sweeps run in: 1,024 FP64, 2,048 FP32).
+template <int D>
+void Engine<D>::build_windows(bool fp32)
+{
+    int want = cell_win_ ? cell_win_ : (fp32 ? 2 * CELL_WIN : CELL_WIN);
+    if (want == win_ && win_valid_) return;
+    int ncol = (int)inv_col_off_.size() - 1;
+    win_ = want;
+    win_off_.assign(ncol + 1, 0);
+    nwin_.assign(ncol, 0);
+    for (int c = 0; c < ncol; c++) {
+        int span = inv_col_off_[c + 1] - inv_col_off_[c];
+        nwin_[c] = act_off_[c + 1] > act_off_[c] ? std::max(1, (span + win_ - 1) / win_) : 0;
+        win_off_[c + 1] = win_off_[c] + nwin_[c] + 1;
+    }
+    wfirst_.reserve((size_t)win_off_[ncol] + 1);
+    for (int c = 0; c < ncol; c++)
+        if (nwin_[c])
+            launch(k_inv_windows, nblk(nwin_[c] + 1, TPB), TPB, 0, st_, act_off_[c], act_off_[c + 1],
+                   (const int *)inv_off_.p, win_, nwin_[c], wfirst_.p + win_off_[c]);
+    win_valid_ = true;
 }
 
 // Mixed form: one ICCG in FP32 (A and the factor rounded to FP32, FP64 dot
@@ -1536,6 +1560,7 @@ void Engine<D>::step_adjoint()
             PcgBufs<double> v{A_.p,      xf_lo_.p, xf_up_.p, pk_val_lo_.p, pk_val_up_.p, dinv_.p, inv_cm_.p,
                               inv_rm_.p, x_.p,     r_.p,     z_.p,         p_.p,         Ap_.p,   y_.p,
                               part_.p,   b_.p};
+            if (icc) build_windows(false);   // FP64 sweeps: FP64 windows
             pcg_solve<double>(v, kAdjRtol, prm_.cg_max_iter, icc, n_eq, nnz_);
             launch(k_adj_mu, RB, CG_BLOCK, 0, st_, n_eq, (const int *)part_of_row_.p, (const int *)S().id,
                    (const double *)x_.p, bnorm, adj_.mu);

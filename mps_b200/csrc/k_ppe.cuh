@@ -674,7 +674,7 @@ constexpr int MBAR_POLLS = 1 << 20;
 // that it overlaps the preceding cross-cell kernel, then its warps take the
 // window's cells in turn.
 
-constexpr int CELL_WIN = 1024;        // default window (entries); MPS_CELL_WIN selects 256..4096
+constexpr int CELL_WIN = 1024;        // default FP64 window (entries; 8 KB); MPS_CELL_WIN selects 256..4096
 constexpr int CELL_WIN_MAX = 4096;
 constexpr int CELL_MAXBLK = ((SWEEP_MAXM * (SWEEP_MAXM + 1) / 2) + 3) & ~3;
 constexpr int CELL_STAGE_MAX = CELL_WIN_MAX + CELL_MAXBLK;
