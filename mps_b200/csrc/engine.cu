@@ -243,7 +243,9 @@ private:
     long long nnz_ = 0;
     int nx_lo_ = 0, nx_up_ = 0;   // entries of the packed cross-cell runs
     int ninv_ = 0;            // entries of the in-cell block inverses
-    int spmv_lpr_ = 8;   // lanes per row of the CG SpMV (MPS_SPMV_LPR: 8, 16 or 32)
+    // lanes per row of the CG SpMV: MPS_SPMV_LPR (8, 16 or 32) if set, else 8
+    // in FP64 and 16 in the mixed form's FP32 solve
+    int spmv_lpr_ = 0;
     // CG-loop kernels launched as programmatic dependents (MPS_PDL_MASK): 2 the
     // colour sweep kernel, 4 SpMV and vector kernels
     int pdl_mask_ = 6;
@@ -1176,12 +1178,13 @@ void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, 
                win_ + CELL_MAXBLK, err_.p);
         }
     };
+    const int lpr = spmv_lpr_ ? spmv_lpr_ : (sizeof(T) == 8 ? 8 : 16);
     auto spmv = [&]() {
         const int *rp = row_ptr_.p, *ci = col_.p;
-        if (spmv_lpr_ == 16)
+        if (lpr == 16)
             lk(4, k_cg_spmv<16, T>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
                ticket_.p, sc_.p);
-        else if (spmv_lpr_ == 32)
+        else if (lpr == 32)
             lk(4, k_cg_spmv<32, T>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
                ticket_.p, sc_.p);
         else

@@ -910,11 +910,13 @@ __device__ __forceinline__ double final_sum(const double *partials, unsigned n, 
     return block_sum<CG_BLOCK>(a, sh);
 }
 
+constexpr int SPMV_U = 8;   // entries per lane loaded in one batch by the FP32 k_cg_spmv
+
 // Ap = A p and the p.Ap partial; the last block forms alpha.  The kernel
 // also performs the loop-head test of the reference (sqrt(r.r) < tol, and
 // the iteration cap) before any work.
 template <int LPR, class T>
-__global__ void k_cg_spmv(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ col,
+__global__ void __launch_bounds__(CG_BLOCK, 8) k_cg_spmv(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ col,
                           const T *__restrict__ A, const T *p, T *Ap,
                           double *partials, unsigned *ticket, CGScalars *sc)
 {
@@ -932,10 +934,30 @@ __global__ void k_cg_spmv(int n_eq, const int *__restrict__ row_ptr, const int *
     for (int rb = blockIdx.x * rows_per_block; rb < n_eq; rb += gridDim.x * rows_per_block) {
         int r = rb + threadIdx.x / LPR;
         T s = T(0);
-        if (r < n_eq) {
+        if (r < n_eq && sizeof(T) == 8) {
             int q1 = __ldg(&row_ptr[r + 1]);
 #pragma unroll 4
             for (int q = __ldg(&row_ptr[r]) + lane; q < q1; q += LPR) s += __ldg(&A[q]) * p[__ldg(&col[q])];
+        } else if (r < n_eq) {
+            // FP32: a lane's first SPMV_U entries are loaded in one batch
+            // (predicated), so a row of up to SPMV_U * LPR nonzeros costs one
+            // round trip for A and col and one for the gathers (an FP32 entry
+            // moves two thirds of an FP64 one per trip); the sum runs in entry
+            // order
+            int q0 = __ldg(&row_ptr[r]) + lane, q1 = __ldg(&row_ptr[r + 1]);
+            T a[SPMV_U];
+            int c[SPMV_U];
+#pragma unroll
+            for (int u = 0; u < SPMV_U; u++) {
+                int q = q0 + u * LPR;
+                bool ok = q < q1;
+                a[u] = ok ? __ldg(&A[q]) : T(0);
+                c[u] = ok ? __ldg(&col[q]) : -1;
+            }
+#pragma unroll
+            for (int u = 0; u < SPMV_U; u++)
+                if (c[u] >= 0) s += a[u] * p[c[u]];
+            for (int q = q0 + SPMV_U * LPR; q < q1; q += LPR) s += __ldg(&A[q]) * p[__ldg(&col[q])];
         }
 #pragma unroll
         for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LPR);
