@@ -25,6 +25,10 @@ per step, and one isolated mps_step_adjoint).
 
 --impl reference times the reference's own CPU implementation (oracle/_ref)
 on the bounded sample, rank 0 only.
+
+--error-growth STEPS prints, instead, the mixed form's long-run accuracy:
+its error growth against the FP64 path next to that of a reordered FP64
+run, and integral observables of the three runs (rank 0, one GPU).
 """
 from __future__ import annotations
 
@@ -498,6 +502,167 @@ def run_e2e(wl, cfg, args, torch, dist):
             "call": "simulation_step(ps, nl, cl, step) of libmps3d.so, pinned host AoS + NeighborList"}
 
 
+# ---- accuracy of the mixed form over a long run ---------------------------------
+#
+# A pointwise comparison of two dam-break runs whose reductions differ stops
+# being meaningful after a few hundred steps (the flow amplifies rounding
+# differences), so the mixed form is reported three ways: its error growth
+# against the FP64 path, next to the growth between two FP64 runs that
+# differ only in the SpMV's summation order (the reordering noise floor), and
+# integral observables of the three runs at the end (fluid count, surge
+# front, pressure binned on a fixed grid and time-averaged, a wall-probe
+# pressure series).
+
+FLUID_T, WALL_T = 0, 1
+
+
+def _rel_l2(a, b):
+    import numpy as np
+    d = float(np.linalg.norm(np.asarray(a, dtype=np.float64) - np.asarray(b, dtype=np.float64)))
+    nb = float(np.linalg.norm(np.asarray(b, dtype=np.float64)))
+    return d / nb if nb > 0 else d
+
+
+def state_errors(a, ref):
+    """Relative L2 differences of one state against a reference state (both
+    particle records in reference order): pressure over all particles,
+    velocity and position over the particles that are fluid in both, and the
+    counts of differing surface flags and types."""
+    import numpy as np
+    both = (a["type"] == FLUID_T) & (ref["type"] == FLUID_T)
+    return {"p_rel": _rel_l2(a["pressure"], ref["pressure"]),
+            "v_rel": _rel_l2(a["vel"][both], ref["vel"][both]),
+            "x_rel": _rel_l2(a["pos"][both], ref["pos"][both]),
+            "surface_flags_differing": int(np.count_nonzero(a["on_surface"] != ref["on_surface"])),
+            "types_differing": int(np.count_nonzero(a["type"] != ref["type"]))}
+
+
+def grid_pressure(state, l0: float, domain, bin_l0: float = 4.0):
+    """Mean fluid pressure per cell of a fixed grid of side bin_l0 * l0 over
+    the tank (x, y, z >= 0 up to `domain`); returns (sum, count) arrays."""
+    import numpy as np
+    h = bin_l0 * l0
+    dims = [max(1, int(np.ceil(domain[d] / h))) for d in range(3)]
+    f = state["type"] == FLUID_T
+    x = state["pos"][f]
+    idx = [np.clip(np.floor(x[:, d] / h).astype(np.int64), 0, dims[d] - 1) for d in range(3)]
+    lin = (idx[0] * dims[1] + idx[1]) * dims[2] + idx[2]
+    tot = dims[0] * dims[1] * dims[2]
+    ssum = np.bincount(lin, weights=state["pressure"][f], minlength=tot)
+    cnt = np.bincount(lin, minlength=tot).astype(np.float64)
+    return ssum, cnt
+
+
+def probe_mask(pos0, types, l0: float, domain, height: float = 0.05, zc: float = 0.15, radius_l0: float = 3.0):
+    """The wall probe: particles of the first wall layer behind the +x wall
+    (x in (Lx, Lx + 1.5 l0)) within radius_l0 * l0 of (height, zc) in the
+    wall's plane (y vertical)."""
+    import numpy as np
+    lx = domain[0]
+    r2 = (pos0[:, 1] - height) ** 2 + (pos0[:, 2] - zc) ** 2
+    return (types == WALL_T) & (pos0[:, 0] > lx) & (pos0[:, 0] < lx + 1.5 * l0) & (r2 <= (radius_l0 * l0) ** 2)
+
+
+def observables(state, probe):
+    """Fluid count, surge front (largest x of a fluid particle) and the mean
+    pressure over the probe particles."""
+    import numpy as np
+    f = state["type"] == FLUID_T
+    return {"fluid": int(np.count_nonzero(f)),
+            "front_x": float(state["pos"][f, 0].max()) if f.any() else 0.0,
+            "probe_p": float(state["pressure"][probe].mean()) if probe.any() else 0.0}
+
+
+def run_error_growth(args):
+    """Mixed form and a reordered FP64 run against the FP64 path over
+    `args.error_growth` steps of the dam break (workload and l0 as given,
+    l0 = 0.01 by default), from the same initial state, in lockstep on one
+    GPU.  Prints one JSON line."""
+    import numpy as np
+    import torch
+
+    from mps_b200 import _lib
+    from mps_b200 import types as T
+    from mps_b200 import workloads as W
+    from mps_b200.session import Session
+
+    steps = int(args.error_growth)
+    l0 = args.l0 if args.l0 is not None else 0.01
+    wl = W.dambreak(args.workload, seed=1000, l0=l0)
+    cfg = wl.config()
+    domain = [cfg.domain_max[d] for d in range(3)]
+    hp = T.HostParticles(3, wl.pos, wl.vel, wl.types)
+
+    def make(prec, lpr):
+        old = os.environ.pop("MPS_SPMV_LPR", None)
+        if lpr:
+            os.environ["MPS_SPMV_LPR"] = str(lpr)
+        try:
+            s = Session(cfg, 3, hp.n, precision=prec)
+        finally:
+            os.environ.pop("MPS_SPMV_LPR", None)
+            if old is not None:
+                os.environ["MPS_SPMV_LPR"] = old
+        s.upload(hp)
+        return s
+
+    runs = {"fp64": make(_lib.PREC_FP64, 8), "mixed": make(_lib.PREC_MIXED, 0),
+            "fp64_reordered": make(_lib.PREC_FP64, 16)}
+    n0, lam, nc = runs["fp64"].compute_initial_params()
+    for s in runs.values():
+        s.set_initial_params(n0, lam, nc)
+        s.neighbor_search()
+    probe = probe_mask(wl.pos, wl.types, l0, domain)
+    marks = sorted({k for k in (1, 10, 50, 100, 200, 300, 400, 500, 600, 700, 800, 900, 1000) if k <= steps} | {steps})
+    growth = {k: {key: [] for key in ("p_rel", "v_rel", "x_rel", "surface_flags_differing", "types_differing")}
+              for k in ("mixed", "fp64_reordered")}
+    obs = {k: [] for k in runs}
+    gsum = {k: None for k in runs}
+    gcnt = {k: None for k in runs}
+    done = 0
+    t0 = time.time()
+    for mk in marks:
+        st = {}
+        for k, s in runs.items():
+            s.step(mk - done)
+            st[k] = s.download().copy()
+        torch.cuda.synchronize()
+        done = mk
+        for k in growth:
+            e = state_errors(st[k], st["fp64"])
+            for key, v in e.items():
+                growth[k][key].append(v)
+        for k in runs:
+            obs[k].append(observables(st[k], probe))
+            if mk >= steps / 2:
+                a, c = grid_pressure(st[k], l0, domain)
+                gsum[k] = a if gsum[k] is None else gsum[k] + a
+                gcnt[k] = c if gcnt[k] is None else gcnt[k] + c
+    wall = time.time() - t0
+    for s in runs.values():
+        s.close()
+    occ = np.ones_like(gcnt["fp64"], dtype=bool)
+    for k in runs:
+        occ &= gcnt[k] > 0
+    gmean = {k: gsum[k][occ] / gcnt[k][occ] for k in runs}
+    series = {k: np.array([o["probe_p"] for o in obs[k]]) for k in runs}
+    final = {k: obs[k][-1] for k in runs}
+    return {
+        "metric": "mixed-form error growth vs FP64 (with the FP64 reordering noise floor)",
+        "workload": wl.name, "particles": int(wl.n), "fluid": int(wl.n_fluid), "steps": steps, "dt": cfg.dt,
+        "checkpoints": marks, "growth": growth,
+        "final_observables": final,
+        "grid_pressure_time_mean_rel_l2": {k: _rel_l2(gmean[k], gmean["fp64"]) for k in ("mixed", "fp64_reordered")},
+        "grid": {"bin": "4 l0", "cells_compared": int(occ.sum()),
+                 "samples": "checkpoints at or after half the run"},
+        "probe": {"particles": int(probe.sum()), "where": "+x wall, y = 0.05 m, z = 0.15 m, radius 3 l0",
+                  "series_fp64": [float(v) for v in series["fp64"]],
+                  "series_rel_l2": {k: _rel_l2(series[k], series["fp64"]) for k in ("mixed", "fp64_reordered")}},
+        "noise_floor_run": "FP64 with the CG SpMV summed over 16 lanes per row instead of 8",
+        "wall_s": wall,
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -512,6 +677,9 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint/forward cost measurement")
     ap.add_argument("--l0", type=float, default=None,
                     help="particle spacing override (smaller cases for profiling)")
+    ap.add_argument("--error-growth", type=int, default=0, metavar="STEPS",
+                    help="instead of the throughput line: the mixed form's error growth against FP64 over "
+                         "STEPS steps (l0 = 0.01 unless --l0), with the FP64 reordering noise floor")
     args = ap.parse_args()
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
@@ -530,6 +698,11 @@ def main():
                                  "sample": meta["sample"]},
                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
+        return 0
+
+    if args.error_growth > 0:
+        if rank == 0:
+            print(json.dumps(run_error_growth(args)))
         return 0
 
     res = run_b200(args, rank, world, local_rank)
