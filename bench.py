@@ -26,6 +26,9 @@ per step, and one isolated mps_step_adjoint).
 --impl reference times the reference's own CPU implementation (oracle/_ref)
 on the bounded sample, rank 0 only.
 
+--sloshing-adjoint STEPS prints, instead, the differentiation form's cost on
+the 3-D sloshing tank with driven walls.
+
 --error-growth STEPS prints, instead, the mixed form's long-run accuracy:
 its error growth against the FP64 path next to that of a reordered FP64
 run, and integral observables of the three runs (rank 0, one GPU).
@@ -663,6 +666,63 @@ def run_error_growth(args):
     }
 
 
+def run_sloshing_adjoint(args):
+    """Cost of the differentiation form on the 3-D sloshing tank with driven
+    walls (tank 0.6 x 0.4 x 0.3 m, y vertical, water depth 0.2 m, l0 = 0.004
+    unless --l0, walls driven along x with A = 0.01 m, f = 1.5 Hz): one
+    rollout of `args.sloshing_adjoint` steps with a checkpoint every
+    `args.every` steps, forward then backward, timed with CUDA events on the
+    library's stream (no warm-up rollout: first-use allocations fall in the
+    forward), the device memory in use after each, and the gradients with
+    respect to the drive amplitude and frequency, the gravity scale, the
+    viscosity and the initial velocities.  Loss: mean squared distance of
+    the fluid positions at the last step to a target shifted by 1 mm."""
+    import numpy as np
+    import torch
+
+    from mps_b200 import _lib
+    from mps_b200 import workloads as W
+    from mps_b200.adjoint import Rollout
+
+    steps, every = int(args.sloshing_adjoint), int(args.every)
+    l0 = args.l0 if args.l0 is not None else 0.004
+    wl = W.sloshing3d(l0=l0, seed=1000, steps=steps)
+    amp, freq, axis = wl.drive
+    cfg = wl.config()
+    prec = _lib.PREC_MIXED if args.precision == "mixed" else _lib.PREC_FP64
+    roll = Rollout(cfg, 3, wl.pos, wl.types, steps, every=every, precision=prec, drive_axis=axis)
+    stream = torch.cuda.ExternalStream(roll.sess.stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    x, u, t = roll.forward(wl.vel, 1.0, cfg.viscosity, amp, freq)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    free, total = torch.cuda.mem_get_info()
+    used_fwd = total - free
+    fl = (t == 0)[:, None]
+    lam = 2.0 * (x - (wl.pos + 0.001)) * fl / max(int(fl.sum()), 1)
+    ev[2].record(stream)
+    dx0, du0, dgs, dnu, dA, df = roll.backward(lam, np.zeros_like(u))
+    ev[3].record(stream)
+    torch.cuda.synchronize()
+    free, total = torch.cuda.mem_get_info()
+    used_bwd = total - free
+    roll.close()
+    fwd = ev[0].elapsed_time(ev[1]) / steps
+    bwd = ev[2].elapsed_time(ev[3]) / steps
+    grads = {"dL_dA": float(dA), "dL_df": float(df), "dL_dgravity_scale": float(dgs), "dL_dnu": float(dnu),
+             "dL_du0_l2": float(np.linalg.norm(du0))}
+    return {"metric": "adjoint/forward cost per step, 3-D sloshing with driven walls",
+            "workload": wl.name, "particles": int(wl.n), "fluid": int(wl.n_fluid), "precision": args.precision,
+            "rollout_steps": steps, "checkpoint_every": every, "dt": cfg.dt, "drive": {"A": amp, "f": freq, "axis": axis},
+            "fwd_ms_per_step": fwd, "backward_ms_per_step": bwd, "adjoint_over_fwd": bwd / fwd,
+            "device_memory_in_use_gb": {"after_forward": used_fwd / 1e9, "after_backward": used_bwd / 1e9},
+            "gradients": grads, "all_finite": bool(np.all(np.isfinite(list(grads.values())))),
+            "note": "backward = segment recompute from each checkpoint + per-step recompute and reverse pass "
+                    "incl. the adjoint PPE solve"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -680,6 +740,10 @@ def main():
     ap.add_argument("--error-growth", type=int, default=0, metavar="STEPS",
                     help="instead of the throughput line: the mixed form's error growth against FP64 over "
                          "STEPS steps (l0 = 0.01 unless --l0), with the FP64 reordering noise floor")
+    ap.add_argument("--sloshing-adjoint", type=int, default=0, metavar="STEPS",
+                    help="instead of the throughput line: adjoint/forward cost of a STEPS-step rollout of the "
+                         "3-D sloshing tank with driven walls (l0 = 0.004 unless --l0)")
+    ap.add_argument("--every", type=int, default=25, help="checkpoint interval of --sloshing-adjoint")
     args = ap.parse_args()
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
@@ -698,6 +762,11 @@ def main():
                                  "sample": meta["sample"]},
                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
+        return 0
+
+    if args.sloshing_adjoint > 0:
+        if rank == 0:
+            print(json.dumps(run_sloshing_adjoint(args)))
         return 0
 
     if args.error_growth > 0:
