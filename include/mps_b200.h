@@ -132,6 +132,10 @@ int  mps_session_destroy(mps_session *s);
 /* Replace the parameters (a changed domain or radius rebuilds the grid and
  * requires a new neighbour search). */
 int  mps_update_params(mps_session *s, const mps_params_t *params);
+/* Select the precision form, MPS_PREC_FP64 or MPS_PREC_MIXED, from the next
+ * step on, every other parameter kept; MPS_ERR_INVALID for any other value.
+ * No counterpart in the reference, whose solver is FP64 only. */
+int  mps_set_precision(mps_session *s, int precision);
 /* Human-readable detail of the session's last failure. */
 const char *mps_last_error(mps_session *s);
 

@@ -99,6 +99,10 @@ void output_vtk(const ParticleSystem *ps, int step, const char *output_dir);
  * mps_dropin_set_exit_on_error(0) and check instead of exiting. */
 int  mps_dropin_last_status(void);
 void mps_dropin_set_exit_on_error(int on);
+/* Not in the reference (FP64 only): the precision form of the drop-in's
+ * steps from the next call on, MPS_PREC_FP64 (default) or MPS_PREC_MIXED;
+ * returns MPS_OK, or MPS_ERR_INVALID for any other value. */
+int  mps_dropin_set_precision(int precision);
 /* Not in the reference: release the device session bound to `ps`. */
 void mps_dropin_release(ParticleSystem *ps);
 

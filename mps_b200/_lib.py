@@ -126,6 +126,7 @@ SIGNATURES = {
     "mps_session_create": (I, [C.POINTER(P), C.POINTER(MpsParams), I]),
     "mps_session_destroy": (I, [P]),
     "mps_update_params": (I, [P, C.POINTER(MpsParams)]),
+    "mps_set_precision": (I, [P, I]),
     "mps_last_error": (C.c_char_p, [P]),
     "mps_upload_particles": (I, [P, P, I]),
     "mps_download_particles": (I, [P, P, I]),

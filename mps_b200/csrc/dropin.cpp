@@ -35,6 +35,7 @@ struct Ctx {
 std::map<const ParticleSystem *, Ctx> g_ctx;
 int g_status = MPS_OK;
 int g_exit_on_error = 1;
+int g_precision = MPS_PREC_FP64;   // mps_dropin_set_precision
 
 void fail(const char *where, int rc, mps_session *s)
 {
@@ -94,7 +95,7 @@ mps_params_t params_from(const SimConfig *c)
     p.cmps_gradient = c->cmps_gradient;
     p.use_analytical_lambda = c->use_analytical_lambda;
     p.hs_mode = c->hs_mode;
-    p.precision = MPS_PREC_FP64;
+    p.precision = g_precision;
     p.refine_tolerance = 1e-10;
     return p;
 }
@@ -194,6 +195,13 @@ extern "C" {
 
 int mps_dropin_last_status(void) { return g_status; }
 void mps_dropin_set_exit_on_error(int on) { g_exit_on_error = on; }
+
+int mps_dropin_set_precision(int precision)
+{
+    if (precision != MPS_PREC_FP64 && precision != MPS_PREC_MIXED) return MPS_ERR_INVALID;
+    g_precision = precision;
+    return MPS_OK;
+}
 
 void mps_dropin_release(ParticleSystem *ps)
 {

@@ -179,6 +179,9 @@ public:
     void get_neighbor_list(int *nb, int *cnt, int max_nb) override;
     void get_cell_index(int *cell) override;
     void get_cell_links(int *head, int *next, int total) override;
+    // the window tables keep the window they were built with (win_), so a
+    // change between the factorisation and the solve stays consistent
+    void set_precision(int precision) override { prm_.precision = precision; }
     void get_ppe(int *eq_idx, int *row_ptr, int *col, double *val, double *b, int *n_eq,
                  long long *nnz) override;
     void run_stage(int stage, const int *nb, const int *cnt, int max_nb, double arg) override;
@@ -1895,6 +1898,12 @@ int mps_update_params(mps_session *s, const mps_params_t *p)
 {
     if (!p) return MPS_ERR_INVALID;
     MPS_API_BODY(s, s->eng->update_params(*p));
+}
+
+int mps_set_precision(mps_session *s, int precision)
+{
+    if (precision != MPS_PREC_FP64 && precision != MPS_PREC_MIXED) return MPS_ERR_INVALID;
+    MPS_API_BODY(s, s->eng->set_precision(precision));
 }
 
 int mps_upload_particles(mps_session *s, const void *particles, int num)

@@ -65,6 +65,7 @@ public:
     virtual void get_neighbor_list(int *nb, int *cnt, int max_nb) = 0;
     virtual void get_cell_index(int *cell) = 0;
     virtual void get_cell_links(int *head, int *next, int total) = 0;
+    virtual void set_precision(int precision) = 0;
     virtual void get_ppe(int *eq_idx, int *row_ptr, int *col, double *val, double *b, int *n_eq,
                          long long *nnz) = 0;
     virtual void run_stage(int stage, const int *nb, const int *cnt, int max_nb, double arg) = 0;

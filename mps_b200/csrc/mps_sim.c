@@ -11,6 +11,7 @@
 #include <string.h>
 #include <sys/stat.h>
 
+#include "../../include/mps_b200.h"
 #include "../../include/mps_dropin.h"
 
 static int skip_line(const char *p)
@@ -72,9 +73,17 @@ static ParticleSystem *load_particles(const char *path)
 
 int main(int argc, char **argv)
 {
-    if (argc < 2) {
-        fprintf(stderr, "Usage: %s <cal_file>\n", argv[0]);
+    if (argc < 2 || argc > 3) {
+        fprintf(stderr, "Usage: %s <cal_file> [fp64|mixed]\n", argv[0]);
         return 1;
+    }
+    /* optional precision form (not in the reference, which is FP64 only) */
+    if (argc == 3) {
+        int prec = strcmp(argv[2], "mixed") == 0 ? MPS_PREC_MIXED : strcmp(argv[2], "fp64") == 0 ? MPS_PREC_FP64 : -1;
+        if (mps_dropin_set_precision(prec) != 0) {
+            fprintf(stderr, "Unknown precision '%s' (fp64 or mixed)\n", argv[2]);
+            return 1;
+        }
     }
     SimConfig config;
     config_set_defaults(&config);

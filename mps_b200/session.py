@@ -84,6 +84,11 @@ class Session:
     def set_initial_params(self, n0: float, lam: float, n0_count: int = 0):
         self._check(self.lib.mps_set_initial_params(self.h, n0, lam, n0_count))
 
+    def set_precision(self, precision: int):
+        """MPS_PREC_FP64 or MPS_PREC_MIXED from the next step on."""
+        self._check(self.lib.mps_set_precision(self.h, int(precision)))
+        self.params.precision = int(precision)
+
     # ---- stepping -------------------------------------------------------------
     def neighbor_search(self):
         self._check(self.lib.mps_neighbor_search(self.h))

@@ -47,3 +47,26 @@ def test_params_struct_matches_config():
     p = _lib.params_from_config(cfg, 3)
     assert p.influence_radius_lap == cfg.influence_radius_lap == 3.1 * 0.02
     assert p.cg_tolerance == 1e-9 and p.solver_type == 1
+
+
+def test_precision_switches_validate_without_gpu():
+    """mps_set_precision rejects a null session and unknown forms; the
+    drop-in's mps_dropin_set_precision accepts the two forms and rejects
+    others; the CLI rejects an unknown precision argument before any GPU
+    work."""
+    import ctypes as C
+    import subprocess
+    from mps_b200 import _lib
+    lib = _lib.load()
+    assert lib.mps_set_precision(None, _lib.PREC_MIXED) == -1
+    assert lib.mps_set_precision(None, 7) == -1
+    drop = C.CDLL(os.path.join(ROOT, "mps_b200", "libmps3d.so"))
+    assert drop.mps_dropin_set_precision(7) == -1
+    assert drop.mps_dropin_set_precision(-1) == -1
+    assert drop.mps_dropin_set_precision(_lib.PREC_MIXED) == 0
+    assert drop.mps_dropin_set_precision(_lib.PREC_FP64) == 0
+    exe = os.path.join(ROOT, "mps_b200", "mps_sim3d")
+    r = subprocess.run([exe, "cal.txt", "double"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "Unknown precision 'double'" in r.stderr
+    r = subprocess.run([exe, "cal.txt", "fp64", "extra"], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "Usage:" in r.stderr

@@ -366,6 +366,38 @@ def test_mixed_precision_against_fp64(steps):
     assert mb["ppe_outer"] >= 1 and mb["converged"] == 1
 
 
+def test_set_precision_switches_the_form():
+    """mps_set_precision: a session created FP64 and switched to the mixed
+    form steps bit for bit like one created mixed; switched back, its next
+    solve is the FP64 one (its pressures leave the mixed run's bits but stay
+    within the mixed form's tolerance); an unknown form is rejected."""
+    _cuda()
+    from mps_b200 import _lib
+    from mps_b200.session import start
+    wl = W.dambreak("c1", l0=0.02, seed=8)
+    cfg = wl.config()
+    h = T.HostParticles(3, wl.pos, wl.vel, wl.types)
+    a = start(cfg, 3, h.copy())
+    b = start(cfg, 3, h.copy(), precision=_lib.PREC_MIXED)
+    a.set_precision(_lib.PREC_MIXED)
+    with pytest.raises(_lib.MpsError) as e:
+        a.set_precision(7)
+    assert e.value.code == -1
+    a.step(2)
+    b.step(2)
+    ga, gb = a.download(), b.download()
+    for f in ("pos", "vel", "pressure", "n", "type", "on_surface"):
+        assert np.array_equal(ga[f], gb[f]), f
+    a.set_precision(_lib.PREC_FP64)
+    a.step(1)
+    b.step(1)
+    ga, gb = a.download(), b.download()
+    a.close()
+    b.close()
+    assert not np.array_equal(ga["pressure"], gb["pressure"])
+    assert _rel(ga["pressure"], gb["pressure"]) < 1e-6
+
+
 _PDL_SCRIPT = r"""
 import sys
 import numpy as np
