@@ -252,6 +252,13 @@ int  mps_state_bytes(mps_session *s, size_t *bytes);
 int  mps_state_save(mps_session *s, void *buf);
 int  mps_state_load(mps_session *s, const void *buf);
 int  mps_adjoint_seed(mps_session *s, const double *lam_pos, const double *lam_vel);
+/* A loss on the pressures a step computes: dLdP (num doubles, reference
+ * particle order; NULL clears) is added to the adjoint of the pressure of
+ * the step that the next mps_step_adjoint reverses, before its adjoint PPE
+ * solve, and is consumed by it.  Pressures that are not PPE unknowns
+ * (surface and dummy particles) carry no gradient.  No counterpart in the
+ * reference. */
+int  mps_adjoint_pressure_seed(mps_session *s, const double *dLdP, int num);
 int  mps_step_adjoint(mps_session *s);
 int  mps_adjoint_get(mps_session *s, double *lam_pos, double *lam_vel, double *grad_gravity,
                      double *grad_viscosity, double *grad_drive);

@@ -152,6 +152,7 @@ SIGNATURES = {
     "mps_state_save": (I, [P, P]),
     "mps_state_load": (I, [P, P]),
     "mps_adjoint_seed": (I, [P, P, P]),
+    "mps_adjoint_pressure_seed": (I, [P, P, I]),
     "mps_step_adjoint": (I, [P]),
     "mps_adjoint_get": (I, [P, P, P, P, P, P]),
 }

@@ -6,7 +6,12 @@ initial geometry; calling it with an initial velocity field ``u0`` (n, dim),
 a gravity scale, a kinematic viscosity and, for driven walls, the drive's
 amplitude and frequency (torch FP64 tensors) runs ``steps`` device-resident
 time steps and returns the final positions and velocities (n, dim) in
-reference order.  Backward runs the hand-written
+reference order.  With ``probe`` (particle indices or a boolean mask in
+reference order, e.g. the wall particles of a pressure probe) it also
+returns the probe's mean pressure after every step, a (steps,) series that
+a loss may use (the sloshing case's time-mean squared wall pressure); its
+adjoint enters each reversed step through mps_adjoint_pressure_seed.
+Backward runs the hand-written
 adjoint kernels of the library (``mps_step_adjoint``) from the last step to
 the first with checkpoint-every-k recomputation: the forward saves the
 state every ``every`` steps; the backward reloads each checkpoint, recomputes
@@ -32,7 +37,7 @@ from .types import HostParticles
 
 class Rollout:
     def __init__(self, cfg, dim: int, pos, types, steps: int, every: int = 1, precision: int = _lib.PREC_FP64,
-                 checkpoint_device: str | None = None, drive_axis: int = 0):
+                 checkpoint_device: str | None = None, drive_axis: int = 0, probe=None):
         if steps < 1 or every < 1:
             raise ValueError("steps and every must be positive")
         self.cfg, self.dim, self.steps, self.every = cfg, dim, int(steps), int(every)
@@ -42,6 +47,13 @@ class Rollout:
         self.sess = Session(cfg, dim, self.n, precision=precision)
         self.g_base = np.array([cfg.gravity[d] for d in range(dim)], dtype=np.float64)
         self.drive_axis = int(drive_axis)
+        self.probe = None
+        if probe is not None:
+            pr = np.asarray(probe)
+            self.probe = np.flatnonzero(pr) if pr.dtype == bool else pr.astype(np.int64).ravel()
+            if self.probe.size == 0:
+                raise ValueError("the probe selects no particle")
+        self.series = np.zeros(0)
         self._upload(np.zeros_like(self.pos))
         self.n0, self.lam, self.n0_count = self.sess.compute_initial_params()
         self.nbytes = self.sess.state_bytes()
@@ -84,16 +96,22 @@ class Rollout:
         self.sess.set_initial_params(self.n0, self.lam, self.n0_count)
         self.sess.neighbor_search()
         self.ckpts = []
+        self.series = np.zeros(self.steps if self.probe is not None else 0)
         for s in range(self.steps):
             if s % self.every == 0:
                 self.ckpts.append(self._save())
             self.sess.step(1)
+            if self.probe is not None:
+                self.series[s] = self.sess.pressure()[self.probe].mean()
         return self._final()
 
-    def backward(self, lam_x: np.ndarray, lam_u: np.ndarray):
-        """Adjoint of the last forward run from the adjoint of (x_T, u_T):
-        returns (dL/dx_0, dL/du_0, dL/d gravity_scale, dL/d viscosity,
-        dL/d drive amplitude, dL/d drive frequency)."""
+    def backward(self, lam_x: np.ndarray, lam_u: np.ndarray, lam_series: np.ndarray | None = None):
+        """Adjoint of the last forward run from the adjoint of (x_T, u_T)
+        and, with a probe, of the probe pressure series: returns (dL/dx_0,
+        dL/du_0, dL/d gravity_scale, dL/d viscosity, dL/d drive amplitude,
+        dL/d drive frequency)."""
+        if lam_series is not None and self.probe is None:
+            raise ValueError("lam_series needs a Rollout with a probe")
         self.sess.adjoint_seed(lam_x, lam_u)
         nseg = len(self.ckpts)
         for seg in reversed(range(nseg)):
@@ -106,6 +124,10 @@ class Rollout:
                 states.append(self._save())
             for k in reversed(range(s1 - s0)):
                 self.sess.state_load(states[k].data_ptr())
+                if lam_series is not None and lam_series[s0 + k] != 0.0:
+                    seed = np.zeros(self.n)
+                    seed[self.probe] = lam_series[s0 + k] / self.probe.size
+                    self.sess.adjoint_pressure_seed(seed)
                 self.sess.step_adjoint()
         lx, lu, gg, gn, gd = self.sess.adjoint_get()
         return lx, lu, float(np.dot(gg, self.g_base)), gn, float(gd[0]), float(gd[1])
@@ -116,7 +138,8 @@ class Rollout:
     def __call__(self, u0: torch.Tensor, gscale: torch.Tensor, nu: torch.Tensor, amp: torch.Tensor | None = None,
                  freq: torch.Tensor | None = None):
         z = torch.zeros((), dtype=torch.float64, device=u0.device)
-        return _RolloutFn.apply(u0, gscale, nu, z if amp is None else amp, z if freq is None else freq, self)
+        out = _RolloutFn.apply(u0, gscale, nu, z if amp is None else amp, z if freq is None else freq, self)
+        return out if self.probe is not None else out[:2]
 
 
 class _RolloutFn(torch.autograd.Function):
@@ -125,14 +148,16 @@ class _RolloutFn(torch.autograd.Function):
         x, u, t = roll.forward(u0.detach().cpu().numpy(), float(gscale), float(nu), float(amp), float(freq))
         ctx.roll = roll
         ctx.dev = u0.device
-        return (torch.from_numpy(x).to(ctx.dev), torch.from_numpy(u).to(ctx.dev))
+        return (torch.from_numpy(x).to(ctx.dev), torch.from_numpy(u).to(ctx.dev),
+                torch.from_numpy(roll.series.copy()).to(ctx.dev))
 
     @staticmethod
-    def backward(ctx, gx, gu):
+    def backward(ctx, gx, gu, gs):
         roll = ctx.roll
         lx = np.zeros((roll.n, roll.dim)) if gx is None else gx.detach().cpu().numpy()
         lu = np.zeros((roll.n, roll.dim)) if gu is None else gu.detach().cpu().numpy()
-        _, du0, dgs, dnu, da, df = roll.backward(lx, lu)
+        ls = None if (gs is None or roll.probe is None) else gs.detach().cpu().numpy()
+        _, du0, dgs, dnu, da, df = roll.backward(lx, lu, ls)
         f64 = dict(dtype=torch.float64, device=ctx.dev)
         return (torch.from_numpy(du0).to(ctx.dev), torch.tensor(dgs, **f64), torch.tensor(dnu, **f64),
                 torch.tensor(da, **f64), torch.tensor(df, **f64), None)

@@ -190,6 +190,7 @@ public:
     void state_save(void *dst) override;
     void state_load(const void *src) override;
     void adjoint_seed(const double *lam_pos, const double *lam_vel) override;
+    void adjoint_pressure_seed(const double *dLdP, int num) override;
     void step_adjoint() override;
     void adjoint_get(double *lam_pos, double *lam_vel, double *grad_gravity, double *grad_viscosity,
                      double *grad_drive) override;
@@ -269,6 +270,8 @@ private:
     // ---- differentiation form (arrays indexed by reference particle index)
     DevArray<double> adjd_, adjsum_;
     DevArray<int> adji_;
+    DevArray<double> pseed_;     // dL/dP of the step the next step_adjoint reverses (reference order)
+    bool pseed_on_ = false;
     DevArray<unsigned char> snap_;           // the step's input state, for the recompute
     Adj<D> adj_{};
     size_t adj_cap_ = 0;
@@ -1487,6 +1490,20 @@ void Engine<D>::adjoint_seed(const double *lam_pos, const double *lam_vel)
 }
 
 template <int D>
+void Engine<D>::adjoint_pressure_seed(const double *dLdP, int num)
+{
+    if (num != n_) throw CudaError("pressure seed size differs from the particle count", MPS_ERR_INVALID);
+    if (!dLdP) {
+        pseed_on_ = false;
+        return;
+    }
+    pseed_.reserve((size_t)cap_ + 1);
+    MPS_CUDA(cudaMemcpyAsync(pseed_.p, dLdP, sizeof(double) * num, cudaMemcpyHostToDevice, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+    pseed_on_ = true;
+}
+
+template <int D>
 void Engine<D>::adjoint_get(double *lam_pos, double *lam_vel, double *grad_gravity, double *grad_viscosity,
                             double *grad_drive)
 {
@@ -1528,6 +1545,8 @@ void Engine<D>::step_adjoint()
         throw CudaError("the adjoint supports hs_mode 0, ppe_type 0, cmps_gradient 0, no clamp",
                         MPS_ERR_UNSUPPORTED);
     ensure_adj();
+    bool pseed = pseed_on_;   // consumed by this call
+    pseed_on_ = false;
     int n = n_;
     if (!n) return;
     int nb = nblk(n, TPB);
@@ -1552,6 +1571,7 @@ void Engine<D>::step_adjoint()
     launch(k_adj_seed<D>, nb, TPB, 0, st_, S(), k_, n, adj_);
     launch(k_adj_pmin<D>, nb, TPB, 0, st_, cells(), S(), k_, n, adj_);
     launch(k_adj_gradient<D>, nb, TPB, 0, st_, cells(), S(), k_, n, adj_);
+    if (pseed) launch(k_adj_add, nb, TPB, 0, st_, n, (const double *)pseed_.p, adj_.lp);
     MPS_CUDA(cudaMemsetAsync(adj_.mu, 0, sizeof(double) * cap_, st_));
     int n_eq = n_eq_;
     if (n_eq > 0) {
@@ -2009,6 +2029,11 @@ int mps_state_bytes(mps_session *s, size_t *bytes)
 int mps_state_save(mps_session *s, void *buf) { MPS_API_BODY(s, s->eng->state_save(buf)); }
 
 int mps_state_load(mps_session *s, const void *buf) { MPS_API_BODY(s, s->eng->state_load(buf)); }
+
+int mps_adjoint_pressure_seed(mps_session *s, const double *dLdP, int num)
+{
+    MPS_API_BODY(s, s->eng->adjoint_pressure_seed(dLdP, num));
+}
 
 int mps_adjoint_seed(mps_session *s, const double *lam_pos, const double *lam_vel)
 {

@@ -75,6 +75,7 @@ public:
     virtual void state_save(void *dst) = 0;
     virtual void state_load(const void *src) = 0;
     virtual void adjoint_seed(const double *lam_pos, const double *lam_vel) = 0;
+    virtual void adjoint_pressure_seed(const double *dLdP, int num) = 0;
     virtual void step_adjoint() = 0;
     virtual void adjoint_get(double *lam_pos, double *lam_vel, double *grad_gravity, double *grad_viscosity,
                              double *grad_drive) = 0;

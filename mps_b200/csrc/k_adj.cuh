@@ -114,6 +114,14 @@ __global__ void k_adj_seed(State<D> s, Consts k, int n, Adj<D> a)
     }
 }
 
+// A loss's own derivative with respect to this step's pressures (reference
+// order), added to the adjoint of P that the gradient stage left.
+__global__ void k_adj_add(int n, const double *__restrict__ src, double *dst)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n) dst[q] += src[q];
+}
+
 // P_min argument (first strictly smaller value in list order, as k_pmin)
 // and, for fluid i, the adjoint that reaches P at that argument:
 //   psc_i = -Kc sum_j phi_ij (e_ij . lap_i),  phi = w / r^2, e_ij = x_j - x_i.

@@ -182,6 +182,15 @@ class Session:
         self._check(self.lib.mps_adjoint_seed(self.h, None if lx is None else lx.ctypes.data,
                                               None if lu is None else lu.ctypes.data))
 
+    def adjoint_pressure_seed(self, dLdP=None):
+        """dL/dP of the pressures computed by the step that the next
+        step_adjoint reverses, (n,) in reference order (None clears)."""
+        if dLdP is None:
+            self._check(self.lib.mps_adjoint_pressure_seed(self.h, None, self.n))
+            return
+        a = np.ascontiguousarray(dLdP, dtype=np.float64).reshape(self.n)
+        self._check(self.lib.mps_adjoint_pressure_seed(self.h, a.ctypes.data, self.n))
+
     def step_adjoint(self):
         self._check(self.lib.mps_step_adjoint(self.h))
 

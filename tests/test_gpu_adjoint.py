@@ -343,6 +343,60 @@ def test_adjoint_drive_gradient():
     roll.close()
 
 
+def test_adjoint_probe_pressure_loss():
+    """A loss on the pressures of every step, the sloshing case's time-mean
+    squared wall-probe pressure (mean over the first wall layer behind the
+    +x wall below y = 0.06 m), through the probe series of Rollout and
+    mps_adjoint_pressure_seed: the loss and its gradients with respect to
+    the drive's amplitude and frequency, the gravity scale and the initial
+    velocities against the dense FP64 autograd of the same driven steps
+    (loss 1e-6, gradients 1e-6 relative)."""
+    _cuda()
+    from mps_b200.adjoint import Rollout
+    from oracle import torch_step as TS
+    wl = _slosh(seed=23)
+    amp, freq, axis = wl.drive
+    cfg = wl.config()
+    l0, lx = cfg.particle_distance, cfg.domain_max[0]
+    probe = (wl.types == 1) & (wl.pos[:, 0] > lx) & (wl.pos[:, 0] < lx + 1.5 * l0) & (wl.pos[:, 1] < 0.06)
+    assert probe.sum() >= 4
+    steps = 4
+    roll = Rollout(cfg, 3, wl.pos, wl.types, steps, every=2, drive_axis=axis, probe=probe)
+    roll.forward(wl.vel, 1.0, cfg.viscosity, amp, freq)
+    ser = roll.series.copy()
+    assert ser.shape == (steps,) and np.any(ser != 0.0)
+    L = float(np.mean(ser ** 2))
+    zero = np.zeros((wl.n, 3))
+    _, du0, dgs, _, dA, dF = roll.backward(zero, zero, 2.0 * ser / steps)
+    roll.close()
+    # the same loss by dense autograd
+    c = TS.consts(cfg, 3, roll.n0, roll.lam)
+    f64 = dict(dtype=torch.float64)
+    u0 = torch.tensor(wl.vel, requires_grad=True, **f64)
+    A = torch.tensor(amp, requires_grad=True, **f64)
+    F = torch.tensor(freq, requires_grad=True, **f64)
+    gs = torch.tensor(1.0, requires_grad=True, **f64)
+    g = torch.tensor([cfg.gravity[d] for d in range(3)], **f64) * gs
+    nu = torch.tensor(cfg.viscosity, **f64)
+    x = torch.tensor(wl.pos, **f64)
+    rest = x.clone()
+    u, key, ty = u0, x.clone(), torch.tensor(wl.types, dtype=torch.int64)
+    pidx = torch.tensor(np.flatnonzero(probe))
+    tl = torch.zeros((), **f64)
+    for k in range(steps):
+        drv = dict(amp=A, freq=F, axis=axis, rest=rest, t1=float(k + 1) * cfg.dt)
+        x, u, key, ty, info = TS.step(x, u, key, ty, g, nu, c, drive=drv)
+        tl = tl + info["P"][pidx].mean() ** 2
+    tl = tl / steps
+    tdu0, tdA, tdF, tdgs = torch.autograd.grad(tl, (u0, A, F, gs))
+    assert abs(L - tl.item()) <= 1e-6 * abs(tl.item())
+    f = wl.types == 0
+    assert _rel(du0[f], tdu0.numpy()[f]) < GRAD_TOL
+    assert abs(dA - float(tdA)) <= GRAD_TOL * abs(float(tdA))
+    assert abs(dF - float(tdF)) <= GRAD_TOL * abs(float(tdF))
+    assert abs(dgs - float(tdgs)) <= GRAD_TOL * abs(float(tdgs))
+
+
 def test_config3_geometry_fd_50_steps():
     """The config-3 set-up at full size (2-D dam break, l0 = 0.005, 6,788
     particles): 50 steps from rest, loss = mean squared distance of the fluid
