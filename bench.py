@@ -9,7 +9,8 @@ and collision, the cell-sort neighbour search, number density and surface
 flags, PPE assembly, IC(0) factorisation and the PCG solve to the absolute
 tolerance 1e-9, the pressure gradient and the correction.  `value` is fluid
 particle-steps/s over all ranks (each rank runs an independent replica with
-its own seed: the path does not shard).  The workload's PPE
+its own seed: the time step has no partition that avoids a halo exchange
+per operator and changes the IC(0) preconditioner).  The workload's PPE
 matrix alone is ~1.5 GB, far above the 126 MB L2, so consecutive steps do
 not run from cache.
 
