@@ -1,6 +1,8 @@
 """CPU checks of the drop-in's host-side functions against the reference
 built from source (oracle/_ref, the reference's own io.c and sim_config.c):
-the deck loaders fill SimConfig byte for byte as the reference's do, and the
+the deck loaders (the drop-in's C ones and the Python package's
+mps_b200.config.load_deck) fill SimConfig byte for byte as the reference's
+do, and the
 CSV and legacy-VTK writers produce byte-identical files, in 3-D and 2-D.
 No GPU is touched: these functions only read and write host memory."""
 import ctypes as C
@@ -9,6 +11,7 @@ import os
 import numpy as np
 import pytest
 
+from mps_b200 import config as CF
 from mps_b200 import types as T
 from mps_b200 import workloads as W
 
@@ -52,7 +55,9 @@ def test_deck_loaders_match_reference(dim, tmp_path):
         assert lib.config_load_cal(cal.encode(), C.byref(cfg)) == 0
         assert lib.config_load_params(cfg.param_file, C.byref(cfg)) == 0
         out.append(bytes(cfg))
+    out.append(bytes(CF.load_deck(cal, dim)))
     assert out[0] == out[1]
+    assert out[2] == out[1]
     cfg = SC.from_buffer_copy(out[0])
     assert cfg.relaxation_coeff == 0.25 and cfg.particle_distance == wl.config().particle_distance
 
