@@ -2,8 +2,8 @@
 built from source (oracle/_ref, the reference's own io.c and sim_config.c):
 the deck loaders (the drop-in's C ones and the Python package's
 mps_b200.config.load_deck) fill SimConfig byte for byte as the reference's
-do, and the
-CSV and legacy-VTK writers produce byte-identical files, in 3-D and 2-D.
+do, and the CSV and legacy-VTK writers produce byte-identical files, in 3-D
+and 2-D.
 No GPU is touched: these functions only read and write host memory."""
 import ctypes as C
 import os
