@@ -366,8 +366,19 @@ int config_load_params(const char *param_path, SimConfig *c)
     return 0;
 }
 
+// The configuration report printed at start-up.  Its text is a user-visible
+// format, kept line for line as the reference prints it (3-D OpenMP
+// sim_config.c:279-334, 2-D sim_config.c:261-322; the two variants differ in
+// labels and in where the surface-tension lines go).
 void config_print(const SimConfig *c)
 {
+    const bool nat_ppe = c->ppe_type == 1, by_count = c->surface_detection_method == 1;
+    const bool st = c->surface_tension_enabled != 0;
+    const char *on_off[2] = {"OFF", "ON"};
+    const char *lambda_src = c->use_analytical_lambda ? "analytical" : "from initial particles";
+    const char *hs = c->hs_mode ? "ON (High order Source term)" : "OFF (standard)";
+    const double col_dist = c->collision_distance_ratio * c->particle_distance;
+
     std::printf("=== Simulation Configuration ===\n");
     std::printf("particle_distance:    %.6f m\n", c->particle_distance);
     std::printf("influence_radius_lap: %.6f m  (ratio = %.2f)  [Laplacian]\n", c->influence_radius_lap,
@@ -376,6 +387,7 @@ void config_print(const SimConfig *c)
                 c->influence_ratio_n);
     std::printf("max_neighbors:        %d\n", c->max_neighbors);
     std::printf("wall_layers:          %d\n", c->wall_layers);
+    std::printf(D == 3 ? "dummy_layers:          %d\n" : "dummy_layers:         %d\n", c->dummy_layers);
     std::printf("density:              %.1f kg/m^3\n", c->density);
     std::printf("viscosity:            %.2e m^2/s\n", c->viscosity);
 #if D == 3
@@ -390,10 +402,45 @@ void config_print(const SimConfig *c)
     std::printf("cg_max_iter:          %d\n", c->cg_max_iter);
     std::printf("cg_tolerance:         %.2e\n", c->cg_tolerance);
     std::printf("relaxation_coeff:     %.4f\n", c->relaxation_coeff);
-    std::printf("clamp_negative_pressure: %s\n", c->clamp_negative_pressure ? "ON" : "OFF");
-    std::printf("ppe_type:             %d\n", c->ppe_type);
+    std::printf("clamp_negative_pressure: %s\n", on_off[c->clamp_negative_pressure ? 1 : 0]);
+#if D == 3
+    std::printf("ppe_type:             %d  (%s)\n", c->ppe_type,
+                nat_ppe ? "Natsui weak-compressible" : "standard density");
+    if (nat_ppe) std::printf("  c_ppe=%.3f  gamma_ppe=%.4f\n", c->c_ppe, c->gamma_ppe);
     std::printf("surface_threshold:    %.4f\n", c->surface_threshold);
-    std::printf("hs_mode:              %d\n", c->hs_mode);
+    std::printf("surface_detection:    %s\n", by_count ? "neighbor count (Natsui)" : "number density");
+    if (by_count) std::printf("  surface_count_threshold=%.3f\n", c->surface_count_threshold);
+    if (st)
+        std::printf("surface_tension:      ON  sigma=%.4e  re_ratio=%.2f  theta_SL=%.1f deg\n",
+                    c->surface_tension_coeff, c->surface_tension_re_ratio, c->wetting_angle_SL);
+    std::printf("restitution_coeff:         %.4f\n", c->restitution_coeff);
+    std::printf("collision_distance_ratio:  %.4f  (col_dist = %.6f m)\n", c->collision_distance_ratio, col_dist);
+    std::printf("domain:               [%.3f, %.3f] x [%.3f, %.3f] x [%.3f, %.3f]\n", c->domain_min[0],
+                c->domain_max[0], c->domain_min[1], c->domain_max[1], c->domain_min[2], c->domain_max[2]);
+    std::printf("cmps_gradient:        %s\n", c->cmps_gradient ? "CMPS (symmetric)" : "standard");
+#else
+    std::printf("ppe_type:             %d  (%s)\n", c->ppe_type, nat_ppe ? "Natsui weakly-compressible" : "density-based");
+    if (nat_ppe) std::printf("  c_ppe = %.4f  gamma_ppe = %.4f\n", c->c_ppe, c->gamma_ppe);
+    std::printf("surface_threshold:    %.4f\n", c->surface_threshold);
+    std::printf("surface_detection_method: %d  (%s)\n", c->surface_detection_method,
+                by_count ? "neighbor_count (Natsui)" : "number_density");
+    if (by_count) std::printf("surface_count_threshold:  %.4f\n", c->surface_count_threshold);
+    std::printf("restitution_coeff:         %.4f\n", c->restitution_coeff);
+    std::printf("collision_distance_ratio:  %.4f  (col_dist = %.6f m)\n", c->collision_distance_ratio, col_dist);
+    std::printf("surface_tension:      %s\n", on_off[st ? 1 : 0]);
+    if (st) {
+        std::printf("  surface_tension_coeff:    %.4f N/m\n", c->surface_tension_coeff);
+        std::printf("  surface_tension_re_ratio: %.2f  (re_st = %.6f m)\n", c->surface_tension_re_ratio,
+                    c->influence_radius_st);
+        std::printf("  wetting_angle_SL:         %.2f deg\n", c->wetting_angle_SL);
+    }
+    std::printf("domain:               [%.3f, %.3f] x [%.3f, %.3f]\n", c->domain_min[0], c->domain_max[0],
+                c->domain_min[1], c->domain_max[1]);
+    std::printf("cmps_gradient:        %d  (%s)\n", c->cmps_gradient,
+                c->cmps_gradient ? "CMPS symmetric (P_i+P_j-P_imin-P_jmin)" : "standard (P_j-P_min)");
+#endif
+    std::printf("use_analytical_lambda: %d  (%s)\n", c->use_analytical_lambda, lambda_src);
+    std::printf("hs_mode:              %d  (%s)\n", c->hs_mode, hs);
     std::printf("output_dir:           %s\n", c->output_dir);
     std::printf("particle_file:        %s\n", c->particle_file);
     std::printf("param_file:           %s\n", c->param_file);

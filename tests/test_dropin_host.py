@@ -83,3 +83,99 @@ def test_writers_match_reference(dim, tmp_path):
     assert len(files[0]) == 2 and files[0].keys() == files[1].keys()
     for f in files[0]:
         assert files[0][f] == files[1][f], f
+
+
+@pytest.mark.parametrize("dim", [3, 2])
+def test_host_helpers_match_reference(dim, capfd):
+    """kernel_weight(_derivative) over r from 0 (below the 0.01 l0 floor)
+    past re, particle_system_create/add (including adds past the capacity),
+    neighbor_list_create / neighbor_get, cell_list_create's grid and
+    config_print's text: the same values and bytes as the reference's."""
+    mine, ref = _libs(dim)
+    SC = T.sim_config_type(dim)
+    CL = T.cell_list_type(dim)
+    PS, NL = C.POINTER(T.ParticleSystem), C.POINTER(T.NeighborList)
+    keep = []
+    for lib in (mine, ref):
+        cfg = SC()
+        lib.config_set_defaults(C.byref(cfg))
+        cfg.particle_distance = 0.01
+        keep.append(cfg)
+        C.c_void_p.in_dll(lib, "g_config").value = C.addressof(cfg)
+        for fn in ("kernel_weight", "kernel_weight_derivative"):
+            getattr(lib, fn).restype = C.c_double
+            getattr(lib, fn).argtypes = [C.c_double, C.c_double]
+        lib.particle_system_create.restype = PS
+        lib.particle_system_create.argtypes = [C.c_int]
+        lib.particle_system_add.argtypes = [PS, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_int]
+        lib.particle_system_free.argtypes = [PS]
+        lib.neighbor_list_create.restype = NL
+        lib.neighbor_list_create.argtypes = [C.c_int, C.c_int]
+        lib.neighbor_list_free.argtypes = [NL]
+        lib.neighbor_get.argtypes = [NL, C.c_int, C.c_int]
+        lib.cell_list_create.restype = C.POINTER(CL)
+        lib.cell_list_create.argtypes = [C.c_int, C.c_double, C.c_void_p, C.c_void_p]
+        lib.cell_list_free.argtypes = [C.POINTER(CL)]
+        lib.config_print.argtypes = [C.POINTER(SC)]
+
+    rs = np.concatenate([[0.0, 1e-6, 1e-4, 0.021, np.nextafter(0.021, 1.0), np.nextafter(0.021, 0.0)],
+                         np.linspace(0.0, 0.04, 401)])
+    for re in (0.021, 0.031):
+        for fn in ("kernel_weight", "kernel_weight_derivative"):
+            a = np.array([getattr(mine, fn)(float(r), re) for r in rs])
+            b = np.array([getattr(ref, fn)(float(r), re) for r in rs])
+            assert np.array_equal(a, b), (fn, re)
+
+    rng = np.random.default_rng(4)
+    pos = rng.normal(size=(8, dim))
+    vel = rng.normal(size=(8, dim))
+    item = T.particle_dtype(dim).itemsize
+    seen = []
+    for lib in (mine, ref):
+        ps = lib.particle_system_create(6)
+        rc = [lib.particle_system_add(ps, (C.c_double * dim)(*pos[k]), (C.c_double * dim)(*vel[k]), k % 4)
+              for k in range(8)]
+        s = ps.contents
+        seen.append((rc, s.num, s.capacity, C.string_at(s.particles, s.num * item)))
+        lib.particle_system_free(ps)
+    assert seen[0] == seen[1]
+    assert seen[0][0] == [0, 1, 2, 3, 4, 5, -1, -1]
+
+    got = []
+    for lib in (mine, ref):
+        nl = lib.neighbor_list_create(5, 8)
+        cnt = [nl.contents.count[i] for i in range(5)]
+        for i in range(5):
+            nl.contents.count[i] = i + 1
+            for j in range(i + 1):
+                nl.contents.neighbors[i * 8 + j] = 100 * i + j
+        got.append((nl.contents.max_neighbors, cnt,
+                    [lib.neighbor_get(nl, i, j) for i in range(5) for j in range(i + 1)]))
+        lib.neighbor_list_free(nl)
+    assert got[0] == got[1] and got[0][1] == [0] * 5
+
+    lo = (C.c_double * dim)(*([-0.013] * dim))
+    hi = (C.c_double * dim)(*[1.6, 0.6, 0.6][:dim])
+    grids = []
+    for lib in (mine, ref):
+        cl = lib.cell_list_create(1000, 0.031, C.cast(lo, C.c_void_p), C.cast(hi, C.c_void_p))
+        c = cl.contents
+        grids.append(tuple(getattr(c, f) for f, _ in CL._fields_ if f not in ("head", "next", "origin"))
+                     + tuple(c.origin))
+        lib.cell_list_free(cl)
+    assert grids[0] == grids[1]
+
+    # the configuration report: defaults, then every optional line switched on
+    libc = C.CDLL(None)
+    for switches in ({}, dict(ppe_type=1, surface_detection_method=1, surface_tension_enabled=1, cmps_gradient=1,
+                              clamp_negative_pressure=1, use_analytical_lambda=1, hs_mode=1,
+                              surface_tension_coeff=0.0728, influence_radius_st=0.031)):
+        texts = []
+        for lib, cfg in zip((mine, ref), keep):
+            for k, v in switches.items():
+                setattr(cfg, k, v)
+            capfd.readouterr()
+            lib.config_print(C.byref(cfg))
+            libc.fflush(None)
+            texts.append(capfd.readouterr().out)
+        assert texts[0] == texts[1] and len(texts[0]) > 200, switches
