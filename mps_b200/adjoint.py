@@ -44,16 +44,23 @@ class Rollout:
         self.pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, dim)
         self.types = np.ascontiguousarray(types, dtype=np.int32)
         self.n = self.types.shape[0]
-        self.sess = Session(cfg, dim, self.n, precision=precision)
-        self.g_base = np.array([cfg.gravity[d] for d in range(dim)], dtype=np.float64)
-        self.drive_axis = int(drive_axis)
         self.probe = None
         if probe is not None:
             pr = np.asarray(probe)
-            self.probe = np.flatnonzero(pr) if pr.dtype == bool else pr.astype(np.int64).ravel()
+            if pr.dtype == bool:
+                if pr.shape != (self.n,):
+                    raise ValueError("a boolean probe needs one entry per particle")
+                self.probe = np.flatnonzero(pr)
+            else:
+                self.probe = pr.astype(np.int64).ravel()
             if self.probe.size == 0:
                 raise ValueError("the probe selects no particle")
+            if self.probe.min() < 0 or self.probe.max() >= self.n:
+                raise ValueError("probe index out of range")
         self.series = np.zeros(0)
+        self.sess = Session(cfg, dim, self.n, precision=precision)
+        self.g_base = np.array([cfg.gravity[d] for d in range(dim)], dtype=np.float64)
+        self.drive_axis = int(drive_axis)
         self._upload(np.zeros_like(self.pos))
         self.n0, self.lam, self.n0_count = self.sess.compute_initial_params()
         self.nbytes = self.sess.state_bytes()

@@ -79,3 +79,13 @@ def test_backward_rejects_series_without_probe():
     r.probe = None
     with pytest.raises(ValueError):
         Rollout.backward(r, np.zeros((2, 3)), np.zeros((2, 3)), np.zeros(4))
+
+
+@pytest.mark.parametrize("probe,msg", [([], "selects no particle"), ([0, 10 ** 9], "out of range"),
+                                       ([-1], "out of range"), (np.zeros(3, dtype=bool), "one entry per particle")])
+def test_probe_validated_before_any_gpu_work(probe, msg):
+    """A bad probe is rejected by the constructor before a session exists."""
+    from mps_b200 import workloads as W
+    wl = W.small_dambreak2d(l0=0.05, seed=1)
+    with pytest.raises(ValueError, match=msg):
+        Rollout(wl.config(), 2, wl.pos, wl.types, steps=2, probe=np.asarray(probe))
