@@ -1,0 +1,32 @@
+"""The reference's own main.c (3-D OpenMP and 2-D variants), compiled
+unchanged against the reference's own headers, links against libmps3d.so /
+libmps2d.so with no missing symbol, loads the B200 libraries and runs up to
+its argument check (no GPU work: without a deck it prints its usage and
+exits 1).  This is the link line a maintainer of the reference uses to swap
+its src/*.c for this library.  Compiled into a temporary directory; skipped
+where the reference sources are absent."""
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.environ.get("MPS_REFERENCE_DIR", "/root/reference")
+
+
+@pytest.mark.parametrize("variant,dim", [("mps_fluid3D_parallel", 3), ("mps_fluid2D", 2)])
+def test_reference_main_links_against_the_dropin(variant, dim, tmp_path):
+    src = os.path.join(REF, variant, "src", "main.c")
+    if not os.path.exists(src):
+        pytest.skip("reference sources absent")
+    lib = os.path.join(ROOT, "mps_b200")
+    exe = str(tmp_path / f"mps_main{dim}d")
+    r = subprocess.run(["gcc", "-O2", "-I", os.path.join(REF, variant, "include"), src, "-L", lib, f"-lmps{dim}d",
+                        f"-Wl,-rpath-link,{lib}", f"-Wl,-rpath,{lib}", "-lm", "-o", exe],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    deps = subprocess.run(["ldd", exe], capture_output=True, text=True, timeout=60).stdout
+    assert os.path.join(lib, f"libmps{dim}d.so") in deps and os.path.join(lib, "libmps_b200.so") in deps, deps
+    assert "not found" not in deps, deps
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 1 and "Usage:" in r.stderr, (r.returncode, r.stderr)
