@@ -423,15 +423,21 @@ def run_e2e(wl, cfg, args, torch, dist):
     the drop-in simulation_step(ps, nl, cl, step) of libmps3d.so, whose
     particles (AoS) and neighbour list live in pinned host memory.  Every
     call copies the particles and the previous step's list to the device and
-    the new particles, list and cell chains back.  Wall-clock per call, max
-    over ranks."""
+    the new particles, list and cell chains back; the drop-in runs the
+    line's precision form (mps_dropin_set_precision).  Timed with CUDA events
+    around the synchronous calls, max over ranks."""
     import numpy as np
 
+    from mps_b200 import _lib
     from mps_b200 import config as CF
     from mps_b200 import types as T
 
     lib = C.CDLL(os.path.join(ROOT, "mps_b200", "libmps3d.so"))
     lib.mps_dropin_set_exit_on_error(0)
+    # the drop-in runs the same precision form as the timed steps
+    prec = _lib.PREC_MIXED if args.precision == "mixed" else _lib.PREC_FP64
+    if lib.mps_dropin_set_precision(prec) != 0:
+        return None
     PS = C.POINTER(T.ParticleSystem)
     NL = C.POINTER(T.NeighborList)
     CLP = C.POINTER(T.CellList3)
@@ -503,7 +509,8 @@ def run_e2e(wl, cfg, args, torch, dist):
     return {"value": whole_job_value(wl.n_fluid, world, steps, wall), "unit": UNIT,
             "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
             "ms_per_step": wall / steps * 1e3,
-            "call": "simulation_step(ps, nl, cl, step) of libmps3d.so, pinned host AoS + NeighborList"}
+            "call": "simulation_step(ps, nl, cl, step) of libmps3d.so, pinned host AoS + NeighborList",
+            "precision": args.precision}
 
 
 # ---- accuracy of the mixed form over a long run ---------------------------------
