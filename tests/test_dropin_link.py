@@ -30,3 +30,26 @@ def test_reference_main_links_against_the_dropin(variant, dim, tmp_path):
     assert "not found" not in deps, deps
     r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "Usage:" in r.stderr, (r.returncode, r.stderr)
+
+
+@pytest.mark.parametrize("variant,dim", [("mps_fluid3D_parallel", 3), ("mps_fluid2D", 2)])
+def test_every_reference_prototype_is_exported(variant, dim):
+    """Every function the reference's public headers declare is exported by
+    the drop-in library of that dimension under the same name."""
+    import glob
+    import re
+    inc = os.path.join(REF, variant, "include")
+    if not os.path.isdir(inc):
+        pytest.skip("reference sources absent")
+    names = set()
+    for h in glob.glob(os.path.join(inc, "*.h")):
+        t = open(h).read()
+        t = re.sub(r"/\*.*?\*/", "", t, flags=re.S)
+        t = re.sub(r"//[^\n]*", "", t)
+        for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b([a-z_][a-z0-9_]*)\s*\([^;{]*\)\s*;", t, flags=re.M):
+            names.add(m.group(1))
+    assert len(names) >= 30
+    nm = subprocess.run(["nm", "-D", "--defined-only", os.path.join(ROOT, "mps_b200", f"libmps{dim}d.so")],
+                        capture_output=True, text=True, timeout=60).stdout.split()
+    exported = set(nm[2::3])
+    assert not (names - exported), sorted(names - exported)
