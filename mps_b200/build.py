@@ -80,8 +80,9 @@ def build_host(force: bool = False, verbose: bool = False) -> list:
     return built
 
 
-def build_oracle() -> None:
-    r = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], capture_output=True, text=True)
+def build_oracle(force: bool = False) -> None:
+    cmd = ["make", "-C", os.path.join(ROOT, "oracle")] + (["-B"] if force else [])
+    r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + r.stdout + r.stderr)
 
@@ -89,7 +90,7 @@ def build_oracle() -> None:
 def build_all(force: bool = False, verbose: bool = False) -> None:
     build_cuda(force=force, verbose=verbose)
     build_host(force=force, verbose=verbose)
-    build_oracle()
+    build_oracle(force=force)
 
 
 if __name__ == "__main__":

@@ -10,8 +10,10 @@ import subprocess
 
 import pytest
 
+from conftest import REF_DIR
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = os.environ.get("MPS_REFERENCE_DIR", "/root/reference")
+REF = REF_DIR or ""
 
 
 @pytest.mark.parametrize("variant,dim", [("mps_fluid3D_parallel", 3), ("mps_fluid2D", 2)])

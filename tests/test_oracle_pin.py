@@ -122,8 +122,8 @@ def test_ppe_matrix_known_answers(oracle3):
 
 
 def test_generator_matches_reference_example_deck():
-    path = os.path.join(REF_DIR, "mps_fluid3D_parallel", "examples", "dambreak", "particles.txt")
-    if not os.path.exists(path):
+    path = os.path.join(REF_DIR or "", "mps_fluid3D_parallel", "examples", "dambreak", "particles.txt")
+    if not REF_DIR or not os.path.exists(path):
         pytest.skip("reference example deck not mounted")
     wl = W.example_dambreak3d()
     lines = [l for l in open(path).read().splitlines() if l and not l.startswith("#")][1:]
