@@ -118,6 +118,14 @@ typedef struct {
     long long prof_iterations;
     long long prof_nnz_sum;           /* sum over profiled iterations of nnz */
     long long prof_rows_sum;          /* sum over profiled iterations of n_eq */
+    /* The last step's PPE solution x against its FP64 matrix and right-hand
+     * side, in both precision forms: ||b - A x||_2 (the true residual, which
+     * the CG loop's recursive residual stops tracking once rounding
+     * dominates), ||b||_2, and the FP64 rounding floor of that residual,
+     * u || |b| + |A| |x| ||_2 with u = 2^-53. */
+    double ppe_true_residual;
+    double ppe_bnorm;
+    double ppe_rounding_floor;
 } mps_metrics_t;
 
 typedef struct mps_session mps_session;

@@ -112,6 +112,9 @@ class MpsMetrics(C.Structure):
         ("prof_iterations", C.c_longlong),
         ("prof_nnz_sum", C.c_longlong),
         ("prof_rows_sum", C.c_longlong),
+        ("ppe_true_residual", C.c_double),
+        ("ppe_bnorm", C.c_double),
+        ("ppe_rounding_floor", C.c_double),
     ]
 
 

@@ -240,7 +240,7 @@ private:
     DevArray<int> ucount_, ucol_, rs_, cell_row0_, row_of_, part_of_row_, rcount_, row_ptr_, diagpos_, col_;
     DevArray<double> A_, F_, b_, x_, r_, z_, p_, Ap_, y_, part_, partials_;
     DevArray<float> A32_, xf32_lo_, xf32_up_, pkv32_lo_, pkv32_up_, inv32_cm_, inv32_rm_, dinv32_;
-    DevArray<float> r32_, z32_, p32_, Ap32_, y32_, part32_, d32_, zprev32_;
+    DevArray<double> zprev_;
     DevArray<CGScalars> sc_;
     DevArray<unsigned> ticket_, err_;
     int n_eq_ = 0;
@@ -308,19 +308,25 @@ private:
     void sort();
     void unsort();
     void ppe(bool clamp);
-    template <class T>
+    // CG buffers: the matrix and the factor stored as TM (double in the FP64
+    // form, float in the mixed form), the vectors always FP64
+    template <class TM>
     struct PcgBufs {
-        const T *A, *xf_lo, *xf_up, *pkv_lo, *pkv_up, *dinv, *inv_cm, *inv_rm;
-        T *x, *r, *z, *p, *Ap, *y, *part;
-        const T *b;
+        const TM *A, *xf_lo, *xf_up, *pkv_lo, *pkv_up, *dinv, *inv_cm, *inv_rm;
+        double *x, *r, *z, *p, *Ap, *y, *part;
+        const double *b;
     };
-    template <class T>
-    void pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, int n_eq, long long nnz,
-                   const T *zprev = nullptr);
+    template <class TM>
+    void pcg_solve(const PcgBufs<TM> &v, double tol, int maxit, bool icc, int n_eq, long long nnz,
+                   const double *zprev = nullptr);
     void mixed_solve(int n_eq, long long nnz, bool icc);
     void build_windows(bool fp32);
     static constexpr int kMaxUpdates = 200;      // reliable updates of the mixed form, at most
-    static constexpr double kDelta = 0.1;        // FP32 residual reduction between reliable updates
+    static constexpr double kDelta = 0.1;        // residual reduction between reliable updates (mixed form)
+    static constexpr double kStall = 0.5;        // a reliable update that does not halve the best true
+    static constexpr int kMaxStalls = 2;         // residual is a stall; this many in a row end the solve
+    static constexpr double kUnitRoundoff = 1.1102230246251565e-16;   // 2^-53
+    static constexpr double kFloor = 0.0;        // mixed form: stop at kFloor * (FP64 rounding floor)
     static constexpr double kAdjRtol = 1.0e-12;  // relative residual of the adjoint PPE solve
     int read_int(const int *dev);
     void check_err();
@@ -993,6 +999,9 @@ void Engine<D>::ppe(bool clamp)
     if (n_eq == 0) {
         met.ppe_iterations = 0;
         met.ppe_residual = 0.0;
+        met.ppe_true_residual = 0.0;
+        met.ppe_bnorm = 0.0;
+        met.ppe_rounding_floor = 0.0;
         met.converged = 1;
         met.nnz = 0;
         MPS_CUDA(cudaEventRecord(ev_[2], st_));
@@ -1121,6 +1130,13 @@ void Engine<D>::ppe(bool clamp)
         met.ppe_residual = std::sqrt(sc_host_->rr);
         met.converged = std::sqrt(sc_host_->rr) < prm_.cg_tolerance;
         met.total_iterations += sc_host_->iter;
+        launch(k_true_residual, RED_BLOCKS, CG_BLOCK, 0, st_, n_eq, (const int *)row_ptr_.p, (const int *)col_.p,
+               (const double *)A_.p, (const double *)x_.p, (const double *)b_.p, partials_.p, ticket_.p, sc_.p);
+        MPS_CUDA(cudaMemcpyAsync(sc_host_, sc_.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, st_));
+        MPS_CUDA(cudaStreamSynchronize(st_));
+        met.ppe_true_residual = std::sqrt(sc_host_->rr_outer);
+        met.ppe_bnorm = std::sqrt(sc_host_->bb);
+        met.ppe_rounding_floor = kUnitRoundoff * std::sqrt(sc_host_->ff);
     }
     launch(k_writeback<D>, nb, TPB, 0, st_, s, row_of_.p, x_.p, n, clamp);
     MPS_CUDA(cudaGetLastError());
@@ -1133,10 +1149,11 @@ void Engine<D>::ppe(bool clamp)
 // the reference's test, or after maxit iterations.  Leaves the final
 // scalars in *sc_host_.
 template <int D>
-template <class T>
-void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, int n_eq, long long nnz,
-                          const T *zprev)
+template <class TM>
+void Engine<D>::pcg_solve(const PcgBufs<TM> &v, double tol, int maxit, bool icc, int n_eq, long long nnz,
+                          const double *zprev)
 {
+    using T = double;
     int ncol = 1 << D;
     const int RB = RED_BLOCKS;
     int iter_before = 0;
@@ -1164,19 +1181,19 @@ void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, 
         const T *rhs = fwdir ? v.r : v.y;
         T *out = fwdir ? v.y : v.z;
         const int *pko = fwdir ? pk_off_lo_.p : pk_off_up_.p, *pkl = fwdir ? pk_len_lo_.p : pk_len_up_.p;
-        const T *pkv = fwdir ? v.pkv_lo : v.pkv_up;
+        const TM *pkv = fwdir ? v.pkv_lo : v.pkv_up;
         const unsigned char *pkk = fwdir ? pk_k_lo_.p : pk_k_up_.p;
         int order[8], nc = 0;
         for (int i = 0; i < ncol; i++) {
             int c = fwdir ? i : ncol - 1 - i;
             if (act_off_[c + 1] > act_off_[c]) order[nc++] = c;
         }
-        auto colk = fwdir ? k_sweep_colour<true, T> : k_sweep_colour<false, T>;
+        auto colk = fwdir ? k_sweep_colour<true, TM> : k_sweep_colour<false, TM>;
         for (int i = 0; i < nc; i++) {
             int c = order[i], cn = i + 1 < nc ? order[i + 1] : -1;
             int nrb = cn >= 0 ? row_off_[cn] : 0, nre = cn >= 0 ? row_off_[cn + 1] : 0;
             int ncb = cn >= 0 ? nblk((long long)(nre - nrb) * 8, CELL_THREADS) : 0;
-            lk(2, colk, nwin_[c] + ncb, CELL_THREADS, sizeof(T) * (win_ + CELL_MAXBLK),
+            lk(2, colk, nwin_[c] + ncb, CELL_THREADS, sizeof(TM) * (win_ + CELL_MAXBLK),
                (const int *)wfirst_.p + win_off_[c], nwin_[c], (const int2 *)adesc_.p, (const int *)inv_off_.p,
                fwdir ? v.inv_cm : v.inv_rm, pko, pkl, pkv, pkk, v.dinv, (const int *)(fwdir ? xp_lo_.p : xp_up_.p),
                (const int *)(fwdir ? xs_lo_.p : xs_up_.p), (const int *)(fwdir ? xc_lo_.p : xc_up_.p),
@@ -1184,17 +1201,17 @@ void Engine<D>::pcg_solve(const PcgBufs<T> &v, double tol, int maxit, bool icc, 
                win_ + CELL_MAXBLK, err_.p);
         }
     };
-    const int lpr = spmv_lpr_ ? spmv_lpr_ : (sizeof(T) == 8 ? 8 : 16);
+    const int lpr = spmv_lpr_ ? spmv_lpr_ : (sizeof(TM) == 8 ? 8 : 16);
     auto spmv = [&]() {
         const int *rp = row_ptr_.p, *ci = col_.p;
         if (lpr == 16)
-            lk(4, k_cg_spmv<16, T>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
+            lk(4, k_cg_spmv<16, TM>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
                ticket_.p, sc_.p);
         else if (lpr == 32)
-            lk(4, k_cg_spmv<32, T>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
+            lk(4, k_cg_spmv<32, TM>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
                ticket_.p, sc_.p);
         else
-            lk(4, k_cg_spmv<8, T>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
+            lk(4, k_cg_spmv<8, TM>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
                ticket_.p, sc_.p);
     };
     if (icc) { sweep(true); sweep(false); }
@@ -1278,12 +1295,13 @@ void Engine<D>::build_windows(bool fp32)
     win_valid_ = true;
 }
 
-// Mixed form: one ICCG in FP32 (A and the factor rounded to FP32, FP64 dot
-// products) with reliable updates.  Whenever its recursive residual has
-// fallen by kDelta since the last update, the FP32 iterate is folded into the
-// FP64 solution, the true residual r = b - A x is recomputed with the FP64
-// matrix, and the iteration resumes from it with its search direction kept.
-// Stops when ||r|| <= max(cg_tolerance, refine_tolerance * ||b||).
+// Mixed form: the ICCG on the FP32-stored matrix and factor (FP64 vectors
+// and arithmetic) with reliable updates.  Whenever the recursive residual
+// has fallen by kDelta since the last update, the true residual r = b - A x
+// is recomputed with the FP64 matrix and the iteration resumes from it with
+// its search direction kept.  Stops when ||b - A x|| <= max(cg_tolerance,
+// refine_tolerance * ||b||, kFloor * u * || |b| + |A| |x| ||) (u the FP64
+// unit roundoff), or when the true residual stalls.
 template <int D>
 void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
 {
@@ -1293,8 +1311,8 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
     xf32_lo_.reserve((size_t)nx_lo_ + 1);
     xf32_up_.reserve((size_t)nx_up_ + 1);
     for (auto *v : {&inv32_cm_, &inv32_rm_}) v->reserve((size_t)ninv_ + 1);
-    for (auto *v : {&dinv32_, &r32_, &z32_, &p32_, &Ap32_, &y32_, &part32_, &d32_, &zprev32_})
-        v->reserve((size_t)cap_);
+    dinv32_.reserve((size_t)cap_);
+    zprev_.reserve((size_t)cap_);
     launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)A_.p, A32_.p);
     if (icc) {
         launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, (size_t)nx_lo_, (const double *)xf_lo_.p,
@@ -1311,43 +1329,49 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
     }
     CGScalars init{};
     MPS_CUDA(cudaMemcpyAsync(sc_.p, &init, sizeof(CGScalars), cudaMemcpyHostToDevice, st_));
-    launch(k_refine_init, RB, CG_BLOCK, 0, st_, n_eq, x_.p, r_.p, r32_.p, (const double *)b_.p, partials_.p,
-           ticket_.p, sc_.p);
+    launch(k_refine_init, RB, CG_BLOCK, 0, st_, n_eq, x_.p, r_.p, (const double *)b_.p, partials_.p, ticket_.p,
+           sc_.p);
     MPS_CUDA(cudaMemcpyAsync(sc_host_, sc_.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, st_));
     MPS_CUDA(cudaStreamSynchronize(st_));
     double bnorm = std::sqrt(sc_host_->rr_outer);
     double rtol = prm_.refine_tolerance > 0.0 ? prm_.refine_tolerance : 1.0e-10;
     double target = std::max(prm_.cg_tolerance, rtol * bnorm);
-    double rnorm = bnorm;
-    int updates = 0;
+    double rnorm = bnorm, rbest = bnorm, floor_norm = 0.0;
+    int updates = 0, stalls = 0;
     PcgBufs<float> v{A32_.p,      xf32_lo_.p, xf32_up_.p, pkv32_lo_.p, pkv32_up_.p, dinv32_.p, inv32_cm_.p,
-                     inv32_rm_.p, d32_.p,     r32_.p,     z32_.p,      p32_.p,      Ap32_.p,   y32_.p,
-                     part32_.p,   r32_.p};
-    const float *zsrc = icc ? z32_.p : r32_.p;   // the preconditioned residual of the FP32 loop
+                     inv32_rm_.p, x_.p,       r_.p,       z_.p,        p_.p,        Ap_.p,     y_.p,
+                     part_.p,     b_.p};
+    const double *zsrc = icc ? z_.p : r_.p;   // the preconditioned residual
     if (rnorm > target) {
         pcg_solve<float>(v, std::max(target, kDelta * rnorm), prm_.cg_max_iter, icc, n_eq, nnz);
         for (;;) {
-            MPS_CUDA(cudaMemcpyAsync(zprev32_.p, zsrc, sizeof(float) * n_eq, cudaMemcpyDeviceToDevice, st_));
-            launch(k_refine_update, RB, CG_BLOCK, 0, st_, n_eq, x_.p, d32_.p);
+            MPS_CUDA(cudaMemcpyAsync(zprev_.p, zsrc, sizeof(double) * n_eq, cudaMemcpyDeviceToDevice, st_));
             launch(k_refine_residual, RB, CG_BLOCK, 0, st_, n_eq, (const int *)row_ptr_.p, (const int *)col_.p,
-                   (const double *)A_.p, (const double *)x_.p, (const double *)b_.p, r_.p, r32_.p, partials_.p,
-                   ticket_.p, sc_.p);
+                   (const double *)A_.p, (const double *)x_.p, (const double *)b_.p, r_.p, partials_.p, ticket_.p,
+                   sc_.p);
             MPS_CUDA(cudaMemcpyAsync(sc_host_, sc_.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, st_));
             MPS_CUDA(cudaStreamSynchronize(st_));
             rnorm = std::sqrt(sc_host_->rr_outer);
+            floor_norm = kUnitRoundoff * std::sqrt(sc_host_->ff);
             updates++;
-            if (rnorm <= target || sc_host_->iter >= prm_.cg_max_iter || sc_host_->breakdown ||
-                updates >= kMaxUpdates)
+            // stagnation: the true residual has stopped falling
+            if (rnorm < kStall * rbest) stalls = 0;
+            else stalls++;
+            rbest = std::min(rbest, rnorm);
+            if (rnorm <= std::max(target, kFloor * floor_norm) || sc_host_->iter >= prm_.cg_max_iter ||
+                sc_host_->breakdown || updates >= kMaxUpdates || stalls >= kMaxStalls)
                 break;
-            pcg_solve<float>(v, std::max(target, kDelta * rnorm), prm_.cg_max_iter, icc, n_eq, nnz,
-                             (const float *)zprev32_.p);
+            pcg_solve<float>(v, std::max(target, kDelta * rnorm), prm_.cg_max_iter, icc, n_eq, nnz, zprev_.p);
         }
     }
     int inner = sc_host_->iter;
     met.ppe_iterations = inner;
     met.ppe_outer = updates;
     met.ppe_residual = rnorm;
-    met.converged = rnorm <= target;
+    met.ppe_true_residual = rnorm;
+    met.ppe_bnorm = bnorm;
+    met.ppe_rounding_floor = floor_norm;
+    met.converged = rnorm <= std::max(target, kFloor * floor_norm);
     met.total_iterations += inner;
 }
 

@@ -27,6 +27,8 @@ struct CGScalars {
     double rz, rr, pAp, alpha, beta, rz_new;
     double tol;
     double rr_outer;        // ||b - A x||^2 of the FP64 refinement (mixed form)
+    double bb;              // ||b||^2 (k_true_residual)
+    double ff;              // || |b| + |A| |x| ||^2 (k_true_residual, k_refine_residual)
     int iter, done, maxit, breakdown;
 };
 
@@ -730,15 +732,16 @@ __global__ void k_gather_colour_offsets(ColourIdx at, int n, const int *__restri
 // dependent: what it loads before pdl_wait() (row bounds, factor values and
 // columns, block inverses, cell descriptors) is written once per step,
 // before the CG loop; x, part and the CG scalars are read only after it.
-template <bool FWD, class T>
+template <bool FWD, class TM>
 __global__ void __launch_bounds__(CELL_THREADS, 6)
 k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict__ desc,
-               const int *__restrict__ inv_off, const T *__restrict__ inv, const int *__restrict__ pk_off,
-               const int *__restrict__ pk_len, const T *__restrict__ pk_val, const unsigned char *__restrict__ pk_k,
-               const T *__restrict__ dinv, const int *__restrict__ xp, const int *__restrict__ xs,
-               const int *__restrict__ xc, const T *__restrict__ xf, int first, int nrb, int nre, const T *rhs,
-               T *part, T *x, const CGScalars *sc, int stage_elems, unsigned *err)
+               const int *__restrict__ inv_off, const TM *__restrict__ inv, const int *__restrict__ pk_off,
+               const int *__restrict__ pk_len, const TM *__restrict__ pk_val, const unsigned char *__restrict__ pk_k,
+               const TM *__restrict__ dinv, const int *__restrict__ xp, const int *__restrict__ xs,
+               const int *__restrict__ xc, const TM *__restrict__ xf, int first, int nrb, int nre, const double *rhs,
+               double *part, double *x, const CGScalars *sc, int stage_elems, unsigned *err)
 {
+    using T = double;   // vectors and sums; TM is the storage type of the factor
     constexpr int LPR = 8;
     extern __shared__ __align__(128) unsigned char cell_stage[];
     __shared__ __align__(8) unsigned long long bar;
@@ -753,13 +756,13 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
             a = FWD ? __ldg(&xp[r]) : __ldg(&xs[r]);
             b = FWD ? __ldg(&xs[r]) : __ldg(&xp[r + 1]);
         }
-        T f[4];
+        TM f[4];
         int cc[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             int q = a + lane + u * LPR;
             bool ok = q < b;
-            f[u] = ok ? __ldg(&xf[q]) : T(0);
+            f[u] = ok ? __ldg(&xf[q]) : TM(0);
             cc[u] = ok ? __ldg(&xc[q]) : -1;
         }
         pdl_wait();
@@ -767,15 +770,15 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
         T s = T(0);
 #pragma unroll
         for (int u = 0; u < 4; u++)
-            if (cc[u] >= 0) s += f[u] * x[cc[u]];
-        for (int q = a + lane + 4 * LPR; q < b; q += LPR) s += __ldg(&xf[q]) * x[__ldg(&xc[q])];
+            if (cc[u] >= 0) s += T(f[u]) * x[cc[u]];
+        for (int q = a + lane + 4 * LPR; q < b; q += LPR) s += T(__ldg(&xf[q])) * x[__ldg(&xc[q])];
 #pragma unroll
         for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LPR);
         if (lane == 0 && r < nre) part[r] = rhs[r] - s;
         return;
     }
     // window CTA
-    T *stage = reinterpret_cast<T *>(cell_stage);
+    TM *stage = reinterpret_cast<TM *>(cell_stage);
     int ka = __ldg(&wfirst[blockIdx.x]), kb = __ldg(&wfirst[blockIdx.x + 1]);
     int o0 = 0, nel = 0, R0 = 0, R1 = 0;
     if (ka < kb) {
@@ -790,7 +793,7 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
     if (threadIdx.x == 0 && staged) mbar_init(b, 1);
     __syncthreads();
     if (threadIdx.x == 0 && staged) {
-        unsigned bytes = (unsigned)nel * (unsigned)sizeof(T);
+        unsigned bytes = (unsigned)nel * (unsigned)sizeof(TM);
         mbar_arrive_expect_tx(b, bytes);
         bulk_g2s(smem_u32(stage), inv + o0, bytes, b);
     }
@@ -807,7 +810,7 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
             if (r < R1) {
                 int a = FWD ? __ldg(&xs[r]) : __ldg(&xp[r]);
                 int e = FWD ? __ldg(&xp[r + 1]) : __ldg(&xs[r]);
-                for (int q = a + lane; q < e; q += TL) s += __ldg(&xf[q]) * x[__ldg(&xc[q])];
+                for (int q = a + lane; q < e; q += TL) s += T(__ldg(&xf[q])) * x[__ldg(&xc[q])];
             }
             s += __shfl_down_sync(0xffffffffu, s, 1, TL);
             if (lane == 0 && r < R1) part[r] = (first ? rhs[r] : part[r]) - s;
@@ -822,20 +825,20 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
     if (nel > stage_elems && threadIdx.x == 0) atomicOr(err, ERR_WINDOW_OVERFLOW);
     if (done) return;
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const T *src = staged ? stage : inv + o0;
+    const TM *src = staged ? stage : inv + o0;
     for (int k = ka + w; k < kb; k += CELL_THREADS / 32) {
         int2 dd = __ldg(&desc[k]);
         int r0 = dd.x, m = dd.y;
-        const T *blk = src + (__ldg(&inv_off[k]) - o0);
+        const TM *blk = src + (__ldg(&inv_off[k]) - o0);
         if (m > SWEEP_MAXM) {
             for (int t = 0; t < m; t++) {
                 int r = FWD ? r0 + t : r0 + m - 1 - t;
                 int po = pk_off[r], l = pk_len[r];
                 T ps = T(0);
-                for (int e = lane; e < l; e += 32) ps += pk_val[po + e] * x[r0 + pk_k[po + e]];
+                for (int e = lane; e < l; e += 32) ps += T(pk_val[po + e]) * x[r0 + pk_k[po + e]];
 #pragma unroll
                 for (int q = 16; q > 0; q >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, q);
-                if (lane == 0) x[r] = (part[r] - ps) * dinv[r];
+                if (lane == 0) x[r] = (part[r] - ps) * T(dinv[r]);
                 __syncwarp();
             }
             continue;
@@ -851,11 +854,11 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
                 T pj = __shfl_sync(0xffffffffu, p0, j);
                 T pk = __shfl_sync(0xffffffffu, p0, kk & 31);
                 if (FWD) {
-                    if (i0 >= j && i0 < m) a0 += blk[tri_colofs(j, m) + i0 - j] * pj;
-                    if (kk < m && i0 >= kk && i0 < m) b0 += blk[tri_colofs(kk, m) + i0 - kk] * pk;
+                    if (i0 >= j && i0 < m) a0 += T(blk[tri_colofs(j, m) + i0 - j]) * pj;
+                    if (kk < m && i0 >= kk && i0 < m) b0 += T(blk[tri_colofs(kk, m) + i0 - kk]) * pk;
                 } else {
-                    if (i0 <= j) a0 += blk[j * (j + 1) / 2 + i0] * pj;
-                    if (kk < m && i0 <= kk) b0 += blk[kk * (kk + 1) / 2 + i0] * pk;
+                    if (i0 <= j) a0 += T(blk[j * (j + 1) / 2 + i0]) * pj;
+                    if (kk < m && i0 <= kk) b0 += T(blk[kk * (kk + 1) / 2 + i0]) * pk;
                 }
             }
         } else {
@@ -864,22 +867,22 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
                 T pj = __shfl_sync(0xffffffffu, j < 32 ? p0 : p1, j & 31);
                 T pk = __shfl_sync(0xffffffffu, kk < 32 ? p0 : p1, kk & 31);
                 if (FWD) {
-                    const T *cj = blk + tri_colofs(j, m) - j;
-                    if (i0 >= j) a0 += cj[i0] * pj;
-                    if (i1 >= j && i1 < m) a1 += cj[i1] * pj;
+                    const TM *cj = blk + tri_colofs(j, m) - j;
+                    if (i0 >= j) a0 += T(cj[i0]) * pj;
+                    if (i1 >= j && i1 < m) a1 += T(cj[i1]) * pj;
                     if (kk < m) {
-                        const T *ck = blk + tri_colofs(kk, m) - kk;
-                        if (i0 >= kk) b0 += ck[i0] * pk;
-                        if (i1 >= kk && i1 < m) b1 += ck[i1] * pk;
+                        const TM *ck = blk + tri_colofs(kk, m) - kk;
+                        if (i0 >= kk) b0 += T(ck[i0]) * pk;
+                        if (i1 >= kk && i1 < m) b1 += T(ck[i1]) * pk;
                     }
                 } else {
-                    const T *rj = blk + j * (j + 1) / 2;
-                    if (i0 <= j) a0 += rj[i0] * pj;
-                    if (i1 <= j) a1 += rj[i1] * pj;
+                    const TM *rj = blk + j * (j + 1) / 2;
+                    if (i0 <= j) a0 += T(rj[i0]) * pj;
+                    if (i1 <= j) a1 += T(rj[i1]) * pj;
                     if (kk < m) {
-                        const T *rk = blk + kk * (kk + 1) / 2;
-                        if (i0 <= kk) b0 += rk[i0] * pk;
-                        if (i1 <= kk) b1 += rk[i1] * pk;
+                        const TM *rk = blk + kk * (kk + 1) / 2;
+                        if (i0 <= kk) b0 += T(rk[i0]) * pk;
+                        if (i1 <= kk) b1 += T(rk[i1]) * pk;
                     }
                 }
             }
@@ -915,11 +918,12 @@ constexpr int SPMV_U = 8;   // entries per lane loaded in one batch by the FP32 
 // Ap = A p and the p.Ap partial; the last block forms alpha.  The kernel
 // also performs the loop-head test of the reference (sqrt(r.r) < tol, and
 // the iteration cap) before any work.
-template <int LPR, class T>
+template <int LPR, class TM>
 __global__ void __launch_bounds__(CG_BLOCK, 8) k_cg_spmv(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ col,
-                          const T *__restrict__ A, const T *p, T *Ap,
+                          const TM *__restrict__ A, const double *p, double *Ap,
                           double *partials, unsigned *ticket, CGScalars *sc)
 {
+    using T = double;   // vectors and sums; TM is the storage type of the matrix
     __shared__ double sh[CG_BLOCK / 32];
     pdl_trigger();
     pdl_wait();
@@ -934,36 +938,36 @@ __global__ void __launch_bounds__(CG_BLOCK, 8) k_cg_spmv(int n_eq, const int *__
     for (int rb = blockIdx.x * rows_per_block; rb < n_eq; rb += gridDim.x * rows_per_block) {
         int r = rb + threadIdx.x / LPR;
         T s = T(0);
-        if (r < n_eq && sizeof(T) == 8) {
+        if (r < n_eq && sizeof(TM) == 8) {
             int q1 = __ldg(&row_ptr[r + 1]);
 #pragma unroll 4
-            for (int q = __ldg(&row_ptr[r]) + lane; q < q1; q += LPR) s += __ldg(&A[q]) * p[__ldg(&col[q])];
+            for (int q = __ldg(&row_ptr[r]) + lane; q < q1; q += LPR) s += T(__ldg(&A[q])) * p[__ldg(&col[q])];
         } else if (r < n_eq) {
-            // FP32: a lane's first SPMV_U entries are loaded in one batch
-            // (predicated), so a row of up to SPMV_U * LPR nonzeros costs one
-            // round trip for A and col and one for the gathers (an FP32 entry
-            // moves two thirds of an FP64 one per trip); the sum runs in entry
-            // order
+            // FP32 matrix: a lane's first SPMV_U entries are loaded in one
+            // batch (predicated), so a row of up to SPMV_U * LPR nonzeros costs
+            // one round trip for A and col and one for the gathers (an FP32
+            // entry moves two thirds of an FP64 one per trip); the sum runs in
+            // entry order, in FP64
             int q0 = __ldg(&row_ptr[r]) + lane, q1 = __ldg(&row_ptr[r + 1]);
-            T a[SPMV_U];
+            TM a[SPMV_U];
             int c[SPMV_U];
 #pragma unroll
             for (int u = 0; u < SPMV_U; u++) {
                 int q = q0 + u * LPR;
                 bool ok = q < q1;
-                a[u] = ok ? __ldg(&A[q]) : T(0);
+                a[u] = ok ? __ldg(&A[q]) : TM(0);
                 c[u] = ok ? __ldg(&col[q]) : -1;
             }
 #pragma unroll
             for (int u = 0; u < SPMV_U; u++)
-                if (c[u] >= 0) s += a[u] * p[c[u]];
-            for (int q = q0 + SPMV_U * LPR; q < q1; q += LPR) s += __ldg(&A[q]) * p[__ldg(&col[q])];
+                if (c[u] >= 0) s += T(a[u]) * p[c[u]];
+            for (int q = q0 + SPMV_U * LPR; q < q1; q += LPR) s += T(__ldg(&A[q])) * p[__ldg(&col[q])];
         }
 #pragma unroll
         for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LPR);
         if (lane == 0 && r < n_eq) {
             Ap[r] = s;
-            acc += (double)p[r] * (double)s;
+            acc += p[r] * s;
         }
     }
     double t = block_sum<CG_BLOCK>(acc, sh);
@@ -1089,8 +1093,8 @@ __global__ void k_convert(size_t n, const S *__restrict__ in, T *__restrict__ ou
         out[i] = (T)in[i];
 }
 
-// x64 = 0, r64 = b, r32 = (float) b, ||b||^2 into sc->rr_outer.
-__global__ void k_refine_init(int n_eq, double *__restrict__ x, double *__restrict__ r, float *__restrict__ r32,
+// x = 0, r = b, ||b||^2 into sc->rr_outer.
+__global__ void k_refine_init(int n_eq, double *__restrict__ x, double *__restrict__ r,
                               const double *__restrict__ b, double *partials, unsigned *ticket, CGScalars *sc)
 {
     __shared__ double sh[CG_BLOCK / 32];
@@ -1099,7 +1103,6 @@ __global__ void k_refine_init(int n_eq, double *__restrict__ x, double *__restri
         double bi = b[i];
         x[i] = 0.0;
         r[i] = bi;
-        r32[i] = (float)bi;
         acc += bi * bi;
     }
     double t = block_sum<CG_BLOCK>(acc, sh);
@@ -1110,20 +1113,11 @@ __global__ void k_refine_init(int n_eq, double *__restrict__ x, double *__restri
     }
 }
 
-// x64 += (double) d32; then the FP64 residual r = b - A x with the FP64
-// matrix, its FP32 copy and ||r||^2 (8 lanes per row).
-__global__ void k_refine_update(int n_eq, double *__restrict__ x, float *__restrict__ d)
-{
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_eq; i += gridDim.x * blockDim.x) {
-        x[i] += (double)d[i];
-        d[i] = 0.0f;
-    }
-}
-
-// Reliable update of the FP32 CG (mixed form): r now holds the FP32 copy of
-// the true FP64 residual and z its preconditioned value; the search
-// direction keeps its history, p = z + beta p_prev with the new z, i.e.
-// p += z - zprev.  New r.z and r.r; the inner loop resumes with `tol`.
+// Reliable update of the CG on the FP32 matrix (mixed form): r now holds
+// the true residual b - A x with the FP64 matrix and z its preconditioned
+// value; the search direction keeps its history, p = z + beta p_prev with
+// the new z, i.e. p += z - zprev.  New r.z and r.r; the loop resumes with
+// `tol`.
 template <class T>
 __global__ void k_reliable_fix(int n_eq, const T *__restrict__ r, const T *__restrict__ z,
                                const T *__restrict__ zprev, T *__restrict__ p, double tol, double *partials,
@@ -1156,37 +1150,115 @@ __global__ void k_reliable_fix(int n_eq, const T *__restrict__ r, const T *__res
     }
 }
 
+// The true residual r = b - A x with the FP64 matrix, ||r||^2 into
+// sc->rr_outer and || |b| + |A| |x| ||^2 into sc->ff (8 lanes per row).
 __global__ void k_refine_residual(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ col,
                                   const double *__restrict__ A, const double *__restrict__ x,
-                                  const double *__restrict__ b, double *__restrict__ r, float *__restrict__ r32,
+                                  const double *__restrict__ b, double *__restrict__ r,
                                   double *partials, unsigned *ticket, CGScalars *sc)
 {
     constexpr int LPR = 8;
     __shared__ double sh[CG_BLOCK / 32];
     int lane = threadIdx.x % LPR;
     int rows_per_block = CG_BLOCK / LPR;
-    double acc = 0.0;
+    double acc = 0.0, accf = 0.0;
     for (int rb = blockIdx.x * rows_per_block; rb < n_eq; rb += gridDim.x * rows_per_block) {
         int i = rb + threadIdx.x / LPR;
-        double s = 0.0;
+        double s = 0.0, sa = 0.0;
         if (i < n_eq) {
             int q1 = __ldg(&row_ptr[i + 1]);
-            for (int q = __ldg(&row_ptr[i]) + lane; q < q1; q += LPR) s += __ldg(&A[q]) * x[__ldg(&col[q])];
+            for (int q = __ldg(&row_ptr[i]) + lane; q < q1; q += LPR) {
+                double t = __ldg(&A[q]) * x[__ldg(&col[q])];
+                s += t;
+                sa += fabs(t);
+            }
         }
 #pragma unroll
-        for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LPR);
+        for (int o = LPR / 2; o > 0; o >>= 1) {
+            s += __shfl_down_sync(0xffffffffu, s, o, LPR);
+            sa += __shfl_down_sync(0xffffffffu, sa, o, LPR);
+        }
         if (lane == 0 && i < n_eq) {
-            double ri = b[i] - s;
+            double bi = b[i];
+            double ri = bi - s;
+            double fi = fabs(bi) + sa;
             r[i] = ri;
-            r32[i] = (float)ri;
             acc += ri * ri;
+            accf += fi * fi;
         }
     }
     double t = block_sum<CG_BLOCK>(acc, sh);
-    if (threadIdx.x == 0) partials[blockIdx.x] = t;
+    double tf = block_sum<CG_BLOCK>(accf, sh);
+    if (threadIdx.x == 0) {
+        partials[2 * blockIdx.x] = t;
+        partials[2 * blockIdx.x + 1] = tf;
+    }
     if (last_block(ticket, gridDim.x)) {
-        double tot = final_sum(partials, gridDim.x, 1, 0, sh);
-        if (threadIdx.x == 0) sc->rr_outer = tot;
+        double tot = final_sum(partials, gridDim.x, 2, 0, sh);
+        double totf = final_sum(partials, gridDim.x, 2, 1, sh);
+        if (threadIdx.x == 0) {
+            sc->rr_outer = tot;
+            sc->ff = totf;
+        }
+    }
+}
+
+// ||b - A x||^2, ||b||^2 and || |b| + |A| |x| ||^2 with the FP64 matrix (8
+// lanes per row), into sc->rr_outer, sc->bb and sc->ff: the true residual of
+// a finished solve, which the recursive residual of the CG loop only tracks
+// until rounding takes over, and the scale of the rounding error of b - A x
+// in FP64 (unit roundoff times the last norm).
+__global__ void k_true_residual(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ col,
+                                const double *__restrict__ A, const double *__restrict__ x,
+                                const double *__restrict__ b, double *partials, unsigned *ticket, CGScalars *sc)
+{
+    constexpr int LPR = 8;
+    __shared__ double sh[CG_BLOCK / 32];
+    int lane = threadIdx.x % LPR;
+    int rows_per_block = CG_BLOCK / LPR;
+    double acc = 0.0, accb = 0.0, accf = 0.0;
+    for (int rb = blockIdx.x * rows_per_block; rb < n_eq; rb += gridDim.x * rows_per_block) {
+        int i = rb + threadIdx.x / LPR;
+        double s = 0.0, sa = 0.0;
+        if (i < n_eq) {
+            int q1 = __ldg(&row_ptr[i + 1]);
+            for (int q = __ldg(&row_ptr[i]) + lane; q < q1; q += LPR) {
+                double t = __ldg(&A[q]) * x[__ldg(&col[q])];
+                s += t;
+                sa += fabs(t);
+            }
+        }
+#pragma unroll
+        for (int o = LPR / 2; o > 0; o >>= 1) {
+            s += __shfl_down_sync(0xffffffffu, s, o, LPR);
+            sa += __shfl_down_sync(0xffffffffu, sa, o, LPR);
+        }
+        if (lane == 0 && i < n_eq) {
+            double bi = b[i];
+            double ri = bi - s;
+            double fi = fabs(bi) + sa;
+            acc += ri * ri;
+            accb += bi * bi;
+            accf += fi * fi;
+        }
+    }
+    double t = block_sum<CG_BLOCK>(acc, sh);
+    double tb = block_sum<CG_BLOCK>(accb, sh);
+    double tf = block_sum<CG_BLOCK>(accf, sh);
+    if (threadIdx.x == 0) {
+        partials[3 * blockIdx.x] = t;
+        partials[3 * blockIdx.x + 1] = tb;
+        partials[3 * blockIdx.x + 2] = tf;
+    }
+    if (last_block(ticket, gridDim.x)) {
+        double tot = final_sum(partials, gridDim.x, 3, 0, sh);
+        double totb = final_sum(partials, gridDim.x, 3, 1, sh);
+        double totf = final_sum(partials, gridDim.x, 3, 2, sh);
+        if (threadIdx.x == 0) {
+            sc->rr_outer = tot;
+            sc->bb = totb;
+            sc->ff = totf;
+        }
     }
 }
 
