@@ -1,7 +1,7 @@
 """Throughput of the MPS time step on B200: one JSON line on rank 0.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload c1] [--precision fp64]
+                    [--workload c2] [--precision both|mixed|fp64]
 
 A step is one full MPS time step (simulation.c:19-118 of the reference) of
 the 3-D dam break named by --workload, device-resident: explicit viscosity
@@ -55,12 +55,16 @@ UNIT = "fluid particle-steps/s"
 WORKLOADS = {
     "c1": "3-D dam break, tank 1.6x0.6x0.6 m, column 0.4x0.6x0.3 m, l0=0.005 m, "
           "1,170,276 particles (576,000 fluid), dt 5e-4, ICCG tol 1e-9",
-    "c2": "3-D dam break, tank 1.6x0.6x0.6 m, column 0.4x0.6x0.3 m, l0=0.0035 m, dt 3.5e-4, ICCG tol 1e-9",
+    "c2": "3-D dam break, tank 1.6x0.6x0.6 m, column 0.4x0.6x0.3 m, l0=0.0035 m, 2,854,670 particles "
+          "(1,656,990 fluid), dt 3.5e-4, ICCG tol 1e-9",
 }
-# The CPU sample: the same dam break at l0 = 0.01 (225,236 particles,
-# 72,000 fluid); one reference step there is a few seconds on 8 cores,
-# against ~80 s at l0 = 0.005.
-CPU_SAMPLE_L0 = 0.01
+# The mixed form's stopping rule, as the engine applies it (engine.cu, mixed_solve).
+MIXED_STOP = ("||b - A x|| <= 4 u || |b| + |A| |x| || (u = 2^-53: four times the rounding floor of an FP64 "
+              "residual, where the FP64 form's solve ends), or two reliable updates in a row that do not halve it")
+# Steps of the reference's CPU build timed by --impl reference: one step of
+# the c2 dam break takes about two minutes on 16 host cores, so the
+# reference arm times a bounded window of the first REF_WINDOW steps.
+REF_WINDOW = 3
 
 
 def _env_int(name, default):
@@ -81,16 +85,17 @@ def host_cores() -> int:
 # CPU: the reference compiled from source (oracle/_ref), bounded sample
 # ---------------------------------------------------------------------------
 
-def reference_cpu_steps(steps: int, warmup: int, l0: float = CPU_SAMPLE_L0, seed: int = 0):
+def reference_cpu_steps(workload: str, steps: int, warmup: int, l0=None, seed: int = 1000):
     """Times `steps` reference simulation_step calls (after `warmup` untimed
-    ones) on the sample; returns (fluid particle-steps/s, seconds/step, meta)."""
+    ones) on the workload (the same seeded initial state as the GPU arm's
+    rank 0); returns (fluid particle-steps/s, seconds/step, meta)."""
     os.environ.setdefault("OMP_NUM_THREADS", str(host_cores()))
     from mps_b200 import config as CF
     from mps_b200 import types as T
     from mps_b200 import workloads as W
     from oracle.pyoracle import Oracle, Reference
 
-    wl = W.dambreak("c1", l0=l0, seed=seed)
+    wl = W.dambreak(workload, l0=l0, seed=seed)
     cfg = wl.config()
     kind = "reference"
     ref = Reference("3d")
@@ -111,9 +116,10 @@ def reference_cpu_steps(steps: int, warmup: int, l0: float = CPU_SAMPLE_L0, seed
     dt = time.perf_counter() - t0
     ref.lib.cell_list_free(cl)
     meta = {"kind": kind, "cores": int(os.environ["OMP_NUM_THREADS"]),
-            "sample": f"c1 geometry at l0={l0} ({wl.n} particles, {wl.n_fluid} fluid), "
-                      f"{steps} reference simulation_step call(s) after {warmup} warm-up, "
-                      "OpenMP build of mps_fluid3D_parallel compiled from source"}
+            "sample": f"{wl.name} ({wl.n} particles, {wl.n_fluid} fluid), the first {steps} reference "
+                      f"simulation_step call(s) from the initial state after {warmup} warm-up, "
+                      "OpenMP build of mps_fluid3D_parallel compiled from source; n0/lambda from the oracle's "
+                      "cell-list form of particle_system_calc_initial_params (bit-identical, not timed)"}
     return wl.n_fluid * steps / dt, dt / max(steps, 1), meta
 
 
@@ -164,7 +170,19 @@ class ClockSampler:
                 if r[5 + k].lower().startswith("active"):
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "sm_samples": sm}
+
+
+def merge_clocks(parts):
+    """One clocks record over several sampled timed regions."""
+    parts = [p for p in parts if p]
+    if not parts:
+        return None
+    sm = [v for p in parts for v in p.get("sm_samples", [])]
+    mx = next((p["sm_max_mhz"] for p in parts if p.get("sm_max_mhz")), None)
+    reasons = sorted({r for p in parts for r in p.get("reasons", [])})
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+            "samples": len(sm), "regions": len(parts)}
 
 
 # ---------------------------------------------------------------------------
@@ -179,10 +197,10 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0}, "fallback"
 
 
-def ncu_traffic(kernel: str):
-    """(DRAM bytes per launch, algorithmic bytes per launch) of `kernel` from
-    the committed ncu summary (profiles/*.md lines
-    'traffic_per_launch_bytes <kernel> <dram bytes> <algorithmic bytes>');
+def ncu_traffic(kernel: str, form: str):
+    """(DRAM bytes, algorithmic bytes) of `kernel` in precision form `form`
+    from a committed ncu summary (profiles/*.md lines
+    'traffic_per_launch_bytes <kernel> <form> <dram bytes> <algorithmic bytes>');
     None when absent.  The bench scales the ratio to its own workload."""
     d = os.path.join(ROOT, "profiles")
     if not os.path.isdir(d):
@@ -192,8 +210,8 @@ def ncu_traffic(kernel: str):
             continue
         for line in open(os.path.join(d, name)):
             t = line.strip().strip("`").split()
-            if len(t) == 4 and t[0] == "traffic_per_launch_bytes" and t[1] == kernel:
-                return float(t[2]), float(t[3])
+            if len(t) == 5 and t[0] == "traffic_per_launch_bytes" and t[1] == kernel and t[2] == form:
+                return float(t[3]), float(t[4])
     return None
 
 
@@ -217,52 +235,43 @@ def whole_job_value(n_fluid_per_rank: int, world: int, steps: int, seconds: floa
     return n_fluid_per_rank * world * steps / seconds
 
 
-def run_b200(args, rank: int, world: int, local_rank: int):
+def time_form(wl, cfg, prec, args, torch, dist, barrier, lib):
+    """Times one precision form on the workload: a session from the initial
+    state, args.warmup untimed steps (the first one's pressures kept for the
+    mixed-vs-FP64 check), then args.steps steps timed with CUDA events on
+    the library's stream (max over ranks), then min(steps, 2) profiled steps
+    (CUDA events around every CG-loop kernel group; not part of the timed
+    figure).  Returns a dict of the form's figures."""
     import numpy as np
-    import torch
 
-    from mps_b200 import _lib
     from mps_b200 import types as T
-    from mps_b200 import workloads as W
     from mps_b200.session import Session
 
-    torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-
-    wl = W.dambreak(args.workload, seed=1000 + rank, l0=args.l0)
-    cfg = wl.config()
-    prec = _lib.PREC_MIXED if args.precision == "mixed" else _lib.PREC_FP64
     hp = T.HostParticles(3, wl.pos, wl.vel, wl.types)
-    sess = Session(cfg, 3, hp.n, precision=prec)
+    sess = Session(cfg, 3, hp.n, precision=prec, refine_tolerance=args.refine_tolerance)
     sess.upload(hp)
     n0, lam, _ = sess.compute_initial_params()
     sess.neighbor_search()
-    for _ in range(args.warmup):
+    sess.step(1)
+    p1 = sess.pressure()
+    for _ in range(args.warmup - 1):
         sess.step(1)
     torch.cuda.synchronize()
     stream = torch.cuda.ExternalStream(sess.stream)
     sess.reset_metrics()
-    clocks = ClockSampler(local_rank) if rank == 0 else None
-    lib = _lib.load()
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    # timed region: K steps, no per-kernel events
+    per_step = []
     barrier()
     torch.cuda.synchronize()
+    clocks = ClockSampler(torch.cuda.current_device()) if args.rank == 0 else None
     l0 = lib.mps_launch_count()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
         sess.step(1)
+        m = sess.metrics()   # host-side copy; each step already ends in a host sync
+        per_step.append((m["ppe_iterations"], m["ppe_true_residual"], m["ppe_bnorm"], m["ppe_rounding_floor"],
+                         m["ppe_outer"]))
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
@@ -270,9 +279,6 @@ def run_b200(args, rank: int, world: int, local_rank: int):
     ms = e0.elapsed_time(e1)
     clk = clocks.stop() if clocks else None
     met = sess.metrics()
-    # kernel breakdown: the next min(K, 2) steps again with CUDA events
-    # around every CG-loop kernel group (they add a little time, so these
-    # steps are not part of `value`)
     sess.reset_metrics()
     sess.set_profiling(True)
     for _ in range(min(args.steps, 2)):
@@ -280,41 +286,138 @@ def run_b200(args, rank: int, world: int, local_rank: int):
     torch.cuda.synchronize()
     pmet = sess.metrics()
     sess.set_profiling(False)
-
-    ms_max = max_over_ranks(ms, dist, "cuda")
-    value = whole_job_value(wl.n_fluid, world, args.steps, ms_max / 1e3)
-    iters = met["total_iterations"]
-
     sess.close()
-    e2e = None if args.no_e2e else run_e2e(wl, cfg, args, torch, dist)
+    ms_max = max_over_ranks(ms, dist, "cuda")
+    it = np.array([r[0] for r in per_step], dtype=np.float64)
+    tr = np.array([r[1] for r in per_step])
+    bn = np.array([r[2] for r in per_step])
+    fl = np.array([r[3] for r in per_step])
+    return {"ms": ms_max, "ms_per_step": ms_max / args.steps, "launches": int(launches), "clocks": clk,
+            "n0": n0, "lambda": lam, "p_step1": p1, "met": met, "pmet": pmet,
+            "iterations_per_step": float(it.mean()), "iterations_total": int(it.sum()),
+            "outer_updates_per_step": float(np.mean([r[4] for r in per_step])),
+            "true_residual": {"mean": float(tr.mean()), "max": float(tr.max()),
+                              "relative_mean": float(np.mean(tr / bn)), "relative_max": float(np.max(tr / bn)),
+                              "over_rounding_floor_mean": float(np.mean(tr / fl))}}
+
+
+def sweep_bytes(pmet, fp32: bool) -> dict:
+    """Algorithmic bytes of one forward and one backward IC(0) sweep (all 8
+    colour launches of k_sweep_colour): every cross-cell factor entry once
+    (value + int32 column), every in-cell block-inverse entry once, and per
+    row the run bounds (2 x 4 B), rhs read, the partial sum written and read
+    back, and the result written (4 x 8 B); the gathers of the solution
+    vector are served on chip."""
+    vb = 4.0 if fp32 else 8.0
+    e = float(pmet["n_eq"])
+    inv = float(pmet["sweep_inverse_entries"])
+    fwd = (vb + 4.0) * pmet["sweep_cross_lo"] + vb * inv + 40.0 * e
+    bwd = (vb + 4.0) * pmet["sweep_cross_up"] + vb * inv + 40.0 * e
+    return {"forward": fwd, "backward": bwd}
+
+
+def run_b200(args, rank: int, world: int, local_rank: int):
+    import numpy as np
+    import torch
+
+    from mps_b200 import _lib
+    from mps_b200 import workloads as W
+
+    torch.cuda.set_device(local_rank)
+    args.rank = rank
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    wl = W.dambreak(args.workload, seed=1000 + rank, l0=args.l0)
+    cfg = wl.config()
+    lib = _lib.load()
+    forms = ["mixed", "fp64"] if args.precision == "both" else [args.precision]
+    res = {}
+    for f in forms:
+        prec = _lib.PREC_MIXED if f == "mixed" else _lib.PREC_FP64
+        res[f] = time_form(wl, cfg, prec, args, torch, dist, barrier, lib)
+    head = forms[0]
+    hr = res[head]
+    value = whole_job_value(wl.n_fluid, world, args.steps, hr["ms"] / 1e3)
+
+    e2e = None if args.no_e2e else run_e2e(wl, cfg, args, torch, dist, head)
     adjoint = None
     if world == 1 and not args.no_adjoint:
-        adjoint = run_adjoint_cost(wl, cfg, prec, torch)
+        adjoint = run_adjoint_cost(wl, cfg, _lib.PREC_MIXED if head == "mixed" else _lib.PREC_FP64, torch)
 
     result = None
     if rank == 0:
         peaks, peak_kind = measured_peaks()
-        nnz_mean = pmet["prof_nnz_sum"] / max(pmet["prof_iterations"], 1)
-        rows_mean = pmet["prof_rows_sum"] / max(pmet["prof_iterations"], 1)
-        # SpMV algorithmic bytes per launch: A value + column 4 B per nonzero,
-        # row pointer 4 B, p and Ap per row (values 8 B in FP64, 4 B in the
-        # mixed form's FP32 inner solve).
-        vb = 8.0 if prec == _lib.PREC_FP64 else 4.0
-        alg_bytes = (vb + 4.0) * nnz_mean + (4.0 + 2.0 * vb) * rows_mean
-        spmv_ms = pmet["prof_spmv_ms"] / max(pmet["prof_spmv_launches"], 1)
-        achieved = alg_bytes / (spmv_ms / 1e3) / 1e9
         peak = float(peaks.get("hbm_gbs", 6650.0))
-        tr = ncu_traffic("k_cg_spmv")
-        traffic = None
-        if tr is not None:
-            traffic = tr[0] / tr[1] * alg_bytes
-        fwd_ms = pmet["prof_fwd_ms"] / max(pmet["prof_fwd_sweeps"], 1)
-        bwd_ms = pmet["prof_bwd_ms"] / max(pmet["prof_bwd_sweeps"], 1)
+        kern = {}
+        roof = []
+        for f in forms:
+            pm = res[f]["pmet"]
+            fp32 = f == "mixed"
+            nnz_mean = pm["prof_nnz_sum"] / max(pm["prof_iterations"], 1)
+            rows_mean = pm["prof_rows_sum"] / max(pm["prof_iterations"], 1)
+            spmv_ms = pm["prof_spmv_ms"] / max(pm["prof_spmv_launches"], 1)
+            fwd_ms = pm["prof_fwd_ms"] / max(pm["prof_fwd_sweeps"], 1)
+            bwd_ms = pm["prof_bwd_ms"] / max(pm["prof_bwd_sweeps"], 1)
+            vec_ms = pm["prof_vec_ms"] / max(pm["prof_iterations"], 1)
+            # SpMV: matrix value + column per nonzero, row pointer, p and Ap per row (FP64)
+            spmv_b = ((4.0 if fp32 else 8.0) + 4.0) * nnz_mean + 20.0 * rows_mean
+            sb = sweep_bytes(pm, fp32)
+            sw_b = 0.5 * (sb["forward"] + sb["backward"])
+            sw_ms = 0.5 * (fwd_ms + bwd_ms)
+            kern[f] = {"k_cg_spmv_ms": spmv_ms, "ic0_forward_sweep_ms(8 colour launches)": fwd_ms,
+                       "ic0_backward_sweep_ms(8 colour launches)": bwd_ms, "cg_axpy_ms": vec_ms}
+            tsw = ncu_traffic("k_sweep_colour", f)
+            tsp = ncu_traffic("k_cg_spmv", f)
+            roof.append({"form": f, "kernel": "k_sweep_colour", "bound": "hbm", "achieved": sw_b / (sw_ms / 1e3) / 1e9,
+                         "peak": peak, "unit": "GB/s", "frac": sw_b / (sw_ms / 1e3) / 1e9 / peak,
+                         "traffic": None if tsw is None else tsw[0] / tsw[1] * sw_b,
+                         "algorithmic_bytes_per_launch": sw_b / 8.0, "launches_per_sweep": 8,
+                         "algorithmic_bytes_per_sweep": sw_b, "ms_per_sweep": sw_ms})
+            roof.append({"form": f, "kernel": "k_cg_spmv", "bound": "hbm", "achieved": spmv_b / (spmv_ms / 1e3) / 1e9,
+                         "peak": peak, "unit": "GB/s", "frac": spmv_b / (spmv_ms / 1e3) / 1e9 / peak,
+                         "traffic": None if tsp is None else tsp[0] / tsp[1] * spmv_b,
+                         "algorithmic_bytes_per_launch": spmv_b, "ms_per_launch": spmv_ms})
+        top = dict(roof[0])
+        top.update({"peak_source": f"{peak_kind} hbm_gbs",
+                    "timing": "CUDA events around every colour sweep (8 launches) and SpMV on the library stream, "
+                              "over min(steps, 2) profiled steps right after the timed region",
+                    "others": roof[1:]})
         cpu = None
         if world == 1 and not args.no_cpu:
-            v, sec, meta = reference_cpu_steps(args.cpu_steps, 0)
+            v, sec, meta = reference_cpu_steps(args.workload, args.cpu_steps, 0, l0=args.l0)
             cpu = {"value": v, "unit": UNIT, "cores": meta["cores"], "kind": meta["kind"], "sample": meta["sample"],
                    "seconds_per_step": sec}
+        forms_out = {}
+        for f in forms:
+            r = res[f]
+            forms_out[f] = {"ms_per_step": r["ms_per_step"],
+                            "fluid_particle_steps_per_s": whole_job_value(wl.n_fluid, world, args.steps,
+                                                                          r["ms"] / 1e3),
+                            "ppe_iterations_per_step": r["iterations_per_step"],
+                            "ppe_iterations_per_s": r["iterations_total"] / (r["ms"] / 1e3),
+                            "reliable_updates_per_step": r["outer_updates_per_step"],
+                            "true_residual": r["true_residual"],
+                            "stage_ms_last_step": {"ops": r["met"]["ms_ops"], "assembly": r["met"]["ms_assembly"],
+                                                   "factor": r["met"]["ms_factor"], "solve": r["met"]["ms_solve"]},
+                            "kernel_ms": kern[f], "gpu_launches": r["launches"], "clocks": r["clocks"]}
+        extra = {}
+        if len(forms) == 2:
+            pm, pf = res["mixed"]["p_step1"], res["fp64"]["p_step1"]
+            extra = {"mixed_over_fp64_speedup": res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"],
+                     "step1_pressure_rel_l2_mixed_vs_fp64": float(np.linalg.norm(pm - pf) / np.linalg.norm(pf)),
+                     "equal_residual": "both forms' true residual ||b - A x|| per step is in forms.*.true_residual; "
+                                       "FP64 stops on the reference's recursive test (sqrt(r.r) < 1e-9), the mixed "
+                                       "form on its true residual (" + MIXED_STOP + ")"}
+        clk_all = [res[f]["clocks"] for f in forms if res[f]["clocks"]]
         result = {
             "metric": METRIC,
             "value": value,
@@ -322,41 +425,36 @@ def run_b200(args, rank: int, world: int, local_rank: int):
             "n_gpus": world,
             "steps": args.steps,
             "warmup": args.warmup,
-            "ms_per_step": ms_max / args.steps,
+            "ms_per_step": hr["ms_per_step"],
             "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f64" if prec == _lib.PREC_FP64 else "f32+f64",
+            "dtype": "f32 storage + f64" if head == "mixed" else "f64",
             "data": "synthetic",
             "config": {
-                "workload": WORKLOADS.get(args.workload, args.workload),
+                "workload": WORKLOADS.get(args.workload, args.workload) if args.l0 is None
+                else f"{args.workload} geometry at l0={args.l0}",
                 "particles_per_gpu": wl.n,
                 "fluid_per_gpu": wl.n_fluid,
-                "precision": args.precision,
+                "precision": head,
+                "forms_timed": forms,
                 "parallelism": f"replicas x{world}",
-                "l2": "inputs larger than L2 (PPE matrix ~1.5 GB per replica)",
-                "n0": n0,
-                "lambda": lam,
+                "l2": "inputs larger than L2 (PPE matrix ~%.1f GB per replica)"
+                      % ((12.0 * hr["met"]["nnz"]) / 1e9),
+                "n0": hr["n0"],
+                "lambda": hr["lambda"],
             },
-            "total_particle_steps_per_s": wl.n * world * args.steps / (ms_max / 1e3),
-            "ppe_iterations_per_step": iters / args.steps,
-            "ppe_iterations_per_s": iters / (ms_max / 1e3),
-            "stage_ms_last_step": {"ops": met["ms_ops"], "assembly": met["ms_assembly"],
-                                   "factor": met["ms_factor"], "solve": met["ms_solve"]},
-            "kernel_ms_per_launch": {"k_cg_spmv": spmv_ms, "ic0_forward_sweep(8 colours)": fwd_ms,
-                                     "ic0_backward_sweep(8 colours)": bwd_ms,
-                                     "cg_vector_kernels_per_iter": pmet["prof_vec_ms"] / max(pmet["prof_iterations"], 1)},
-            "roofline": {"kernel": "k_cg_spmv", "bound": "hbm", "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": f"{peak_kind} hbm_gbs",
-                         "timing": "CUDA events around every SpMV launch on the library stream, over "
-                                   "min(steps, 2) further steps right after the timed region",
-                         "algorithmic_bytes_per_launch": alg_bytes},
+            "total_particle_steps_per_s": wl.n * world * args.steps / (hr["ms"] / 1e3),
+            "ppe_iterations_per_step": hr["iterations_per_step"],
+            "ppe_iterations_per_s": hr["iterations_total"] / (hr["ms"] / 1e3),
+            "forms": forms_out,
+            **extra,
+            "roofline": top,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "adjoint": adjoint,
-            "gpu_launches": int(launches),
-            "clocks": clk,
+            "gpu_launches": int(hr["launches"]),
+            "clocks": merge_clocks(clk_all),
         }
     if dist is not None:
         dist.destroy_process_group()
@@ -418,7 +516,7 @@ def run_adjoint_cost(wl, cfg, prec, torch, steps: int = 2):
                     "PPE solve; loss = mean squared distance of fluid positions to a shifted target"}
 
 
-def run_e2e(wl, cfg, args, torch, dist):
+def run_e2e(wl, cfg, args, torch, dist, form):
     """The same metric through the reference-facing C ABI with host buffers:
     the drop-in simulation_step(ps, nl, cl, step) of libmps3d.so, whose
     particles (AoS) and neighbour list live in pinned host memory.  Every
@@ -435,7 +533,7 @@ def run_e2e(wl, cfg, args, torch, dist):
     lib = C.CDLL(os.path.join(ROOT, "mps_b200", "libmps3d.so"))
     lib.mps_dropin_set_exit_on_error(0)
     # the drop-in runs the same precision form as the timed steps
-    prec = _lib.PREC_MIXED if args.precision == "mixed" else _lib.PREC_FP64
+    prec = _lib.PREC_MIXED if form == "mixed" else _lib.PREC_FP64
     if lib.mps_dropin_set_precision(prec) != 0:
         return None
     PS = C.POINTER(T.ParticleSystem)
@@ -510,7 +608,7 @@ def run_e2e(wl, cfg, args, torch, dist):
             "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps,
             "ms_per_step": wall / steps * 1e3,
             "call": "simulation_step(ps, nl, cl, step) of libmps3d.so, pinned host AoS + NeighborList",
-            "precision": args.precision}
+            "precision": form}
 
 
 # ---- accuracy of the mixed form over a long run ---------------------------------
@@ -699,7 +797,7 @@ def run_sloshing_adjoint(args):
     wl = W.sloshing3d(l0=l0, seed=1000, steps=steps)
     amp, freq, axis = wl.drive
     cfg = wl.config()
-    prec = _lib.PREC_MIXED if args.precision == "mixed" else _lib.PREC_FP64
+    prec = _lib.PREC_FP64 if args.precision == "fp64" else _lib.PREC_MIXED
     domain = [cfg.domain_max[d] for d in range(3)]
     probe = probe_mask(wl.pos, wl.types, l0, domain, height=0.1, zc=0.5 * domain[2])
     roll = Rollout(cfg, 3, wl.pos, wl.types, steps, every=every, precision=prec, drive_axis=axis, probe=probe)
@@ -726,7 +824,8 @@ def run_sloshing_adjoint(args):
     grads = {"dL_dA": float(dA), "dL_df": float(df), "dL_dgravity_scale": float(dgs), "dL_dnu": float(dnu),
              "dL_du0_l2": float(np.linalg.norm(du0))}
     return {"metric": "adjoint/forward cost per step, 3-D sloshing with driven walls",
-            "workload": wl.name, "particles": int(wl.n), "fluid": int(wl.n_fluid), "precision": args.precision,
+            "workload": wl.name, "particles": int(wl.n), "fluid": int(wl.n_fluid),
+            "precision": "fp64" if args.precision == "fp64" else "mixed",
             "rollout_steps": steps, "checkpoint_every": every, "dt": cfg.dt, "drive": {"A": amp, "f": freq, "axis": axis},
             "fwd_ms_per_step": fwd, "backward_ms_per_step": bwd, "adjoint_over_fwd": bwd / fwd,
             "device_memory_in_use_gb": {"after_forward": used_fwd / 1e9, "after_backward": used_bwd / 1e9},
@@ -743,8 +842,11 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"],
+                    help="both: the mixed form (value) and the FP64 form timed on the same workload")
+    ap.add_argument("--refine-tolerance", type=float, default=0.0,
+                    help="mixed form: also stop at ||b - A x|| <= this * ||b|| (0: off)")
     ap.add_argument("--cpu-steps", type=int, default=1)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -766,11 +868,16 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        v, sec, meta = reference_cpu_steps(args.steps, args.warmup)
+        nsteps = min(args.steps, REF_WINDOW)
+        v, sec, meta = reference_cpu_steps(args.workload, nsteps, 0, l0=args.l0)
+        meta["sample"] += (f"; a bounded window of {nsteps} step(s) instead of {args.steps} after {args.warmup} "
+                           "warm-up (no warm-up: the reference allocates its PPE buffers in every call)")
         line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-                "config": {"workload": WORKLOADS[args.workload] + "; timed on the CPU sample below",
+                "same_config": True, "timed_steps": nsteps,
+                "config": {"workload": WORKLOADS[args.workload] if args.l0 is None
+                           else f"{args.workload} geometry at l0={args.l0}",
                            "precision": "fp64", "parallelism": "OpenMP, host cores"},
                 "cpu_baseline": {"value": v, "unit": UNIT, "cores": meta["cores"], "kind": meta["kind"],
                                  "sample": meta["sample"]},

@@ -36,7 +36,9 @@ extern "C" {
 
 /* Precision forms of the step. */
 #define MPS_PREC_FP64  0   /* the reference's arithmetic, FP64 everywhere */
-#define MPS_PREC_MIXED 1   /* FP32 operators/SpMV/IC(0), FP64 dots, refinement, integration */
+#define MPS_PREC_MIXED 1   /* PPE matrix and IC(0) factor stored in FP32 (SpMV in difference
+                              form), FP64 vectors, dot products, refinement residuals and
+                              everything outside the PPE solve */
 
 /* PPE unknown orderings for the IC(0) preconditioner. */
 #define MPS_ORDER_BLOCK_COLOR 0  /* cells as blocks, 2^dim colours (default) */
@@ -76,7 +78,9 @@ typedef struct {
     int    hs_mode;
     int    precision;                 /* MPS_PREC_* */
     double refine_tolerance;          /* mixed form: stop at ||b - A x|| <= max(cg_tolerance,
-                                         refine_tolerance * ||b||) (0 = 1e-10) */
+                                         refine_tolerance * ||b||, 4 u || |b| + |A| |x| ||),
+                                         u = 2^-53: the last term is where FP64 residuals
+                                         bottom out (0: that term alone decides) */
     /* Driven walls (no counterpart in the reference, whose walls never move):
      * every WALL and DUMMY particle follows x_axis = rest + A sin(2 pi f t),
      * u_axis = 2 pi f A cos(2 pi f t), rest = its position at upload, t the
@@ -126,6 +130,12 @@ typedef struct {
     double ppe_true_residual;
     double ppe_bnorm;
     double ppe_rounding_floor;
+    /* Sizes of the last step's IC(0) sweep data: cross-cell entries of the
+     * factor read by the forward and the backward sweep, and the entries of
+     * the in-cell block inverses (read once per sweep). */
+    long long sweep_cross_lo;
+    long long sweep_cross_up;
+    long long sweep_inverse_entries;
 } mps_metrics_t;
 
 typedef struct mps_session mps_session;

@@ -115,6 +115,9 @@ class MpsMetrics(C.Structure):
         ("ppe_true_residual", C.c_double),
         ("ppe_bnorm", C.c_double),
         ("ppe_rounding_floor", C.c_double),
+        ("sweep_cross_lo", C.c_longlong),
+        ("sweep_cross_up", C.c_longlong),
+        ("sweep_inverse_entries", C.c_longlong),
     ]
 
 
@@ -188,7 +191,7 @@ class MpsError(RuntimeError):
         super().__init__(f"{ERRORS.get(code, code)}: {what}")
 
 
-def params_from_config(cfg, dim: int, precision: int = PREC_FP64, refine_tolerance: float = 1e-10) -> MpsParams:
+def params_from_config(cfg, dim: int, precision: int = PREC_FP64, refine_tolerance: float = 0.0) -> MpsParams:
     """The session parameters of a reference ``SimConfig`` (already parsed)."""
     p = MpsParams()
     p.dim = dim

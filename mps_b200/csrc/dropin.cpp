@@ -96,7 +96,7 @@ mps_params_t params_from(const SimConfig *c)
     p.use_analytical_lambda = c->use_analytical_lambda;
     p.hs_mode = c->hs_mode;
     p.precision = g_precision;
-    p.refine_tolerance = 1e-10;
+    p.refine_tolerance = 0.0;
     return p;
 }
 

@@ -240,7 +240,7 @@ private:
     DevArray<int> ucount_, ucol_, rs_, cell_row0_, row_of_, part_of_row_, rcount_, row_ptr_, diagpos_, col_;
     DevArray<double> A_, F_, b_, x_, r_, z_, p_, Ap_, y_, part_, partials_;
     DevArray<float> A32_, xf32_lo_, xf32_up_, pkv32_lo_, pkv32_up_, inv32_cm_, inv32_rm_, dinv32_;
-    DevArray<double> zprev_;
+    DevArray<double> zprev_, dsum_;
     DevArray<CGScalars> sc_;
     DevArray<unsigned> ticket_, err_;
     int n_eq_ = 0;
@@ -250,6 +250,11 @@ private:
     // lanes per row of the CG SpMV: MPS_SPMV_LPR (8, 16 or 32) if set, else 8
     // in FP64 and 16 in the mixed form's FP32 solve
     int spmv_lpr_ = 0;
+    // mixed form: residual reduction between reliable updates (MPS_RELIABLE_DELTA
+    // overrides) and the SpMV of its inner loop (MPS_MIXED_SPMV): 0 the FP32
+    // copy of A, 1 the FP64 matrix, 2 the FP32 copy in difference form
+    double rel_delta_ = kDelta;
+    int mixed_spmv_ = 2;
     // CG-loop kernels launched as programmatic dependents (MPS_PDL_MASK): 2 the
     // colour sweep kernel, 4 SpMV and vector kernels
     int pdl_mask_ = 6;
@@ -315,6 +320,8 @@ private:
         const TM *A, *xf_lo, *xf_up, *pkv_lo, *pkv_up, *dinv, *inv_cm, *inv_rm;
         double *x, *r, *z, *p, *Ap, *y, *part;
         const double *b;
+        const double *A64 = nullptr;   // if set, the SpMV reads this FP64 matrix instead of A
+        const double *dsum = nullptr;  // if set, the SpMV is in difference form with these row sums
     };
     template <class TM>
     void pcg_solve(const PcgBufs<TM> &v, double tol, int maxit, bool icc, int n_eq, long long nnz,
@@ -322,11 +329,11 @@ private:
     void mixed_solve(int n_eq, long long nnz, bool icc);
     void build_windows(bool fp32);
     static constexpr int kMaxUpdates = 200;      // reliable updates of the mixed form, at most
-    static constexpr double kDelta = 0.1;        // residual reduction between reliable updates (mixed form)
+    static constexpr double kDelta = 0.01;       // residual reduction between reliable updates (mixed form)
     static constexpr double kStall = 0.5;        // a reliable update that does not halve the best true
     static constexpr int kMaxStalls = 2;         // residual is a stall; this many in a row end the solve
     static constexpr double kUnitRoundoff = 1.1102230246251565e-16;   // 2^-53
-    static constexpr double kFloor = 0.0;        // mixed form: stop at kFloor * (FP64 rounding floor)
+    static constexpr double kFloor = 4.0;        // mixed form: stop at kFloor * (FP64 rounding floor)
     static constexpr double kAdjRtol = 1.0e-12;  // relative residual of the adjoint PPE solve
     int read_int(const int *dev);
     void check_err();
@@ -356,6 +363,11 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
         if (v == 8 || v == 16 || v == 32) spmv_lpr_ = v;
     }
     if (const char *e = std::getenv("MPS_PDL_MASK")) pdl_mask_ = std::atoi(e) & 7;
+    if (const char *e = std::getenv("MPS_RELIABLE_DELTA")) {
+        double v = std::atof(e);
+        if (v > 0.0 && v < 1.0) rel_delta_ = v;
+    }
+    if (const char *e = std::getenv("MPS_MIXED_SPMV")) mixed_spmv_ = std::atoi(e);
     if (const char *e = std::getenv("MPS_CELL_WIN")) {
         int v = std::atoi(e);
         if (v >= 256 && v <= CELL_WIN_MAX && v % 4 == 0) cell_win_ = v;
@@ -1115,6 +1127,9 @@ void Engine<D>::ppe(bool clamp)
                    inv_cm_.p, inv_rm_.p);
         win_valid_ = false;
         build_windows(prm_.precision == MPS_PREC_MIXED);
+        met.sweep_cross_lo = nx_lo_;
+        met.sweep_cross_up = nx_up_;
+        met.sweep_inverse_entries = ninv_;
     }
     MPS_CUDA(cudaEventRecord(ev_[3], st_));
 
@@ -1204,15 +1219,24 @@ void Engine<D>::pcg_solve(const PcgBufs<TM> &v, double tol, int maxit, bool icc,
     const int lpr = spmv_lpr_ ? spmv_lpr_ : (sizeof(TM) == 8 ? 8 : 16);
     auto spmv = [&]() {
         const int *rp = row_ptr_.p, *ci = col_.p;
-        if (lpr == 16)
+        if (v.A64)
+            lk(4, k_cg_spmv<8, double>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A64, (const T *)v.p, v.Ap, partials_.p,
+               ticket_.p, sc_.p, (const double *)nullptr);
+        else if (v.dsum && lpr == 16)
+            lk(4, k_cg_spmv<16, TM, true>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
+               ticket_.p, sc_.p, v.dsum);
+        else if (v.dsum)
+            lk(4, k_cg_spmv<8, TM, true>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
+               ticket_.p, sc_.p, v.dsum);
+        else if (lpr == 16)
             lk(4, k_cg_spmv<16, TM>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
-               ticket_.p, sc_.p);
+               ticket_.p, sc_.p, (const double *)nullptr);
         else if (lpr == 32)
             lk(4, k_cg_spmv<32, TM>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
-               ticket_.p, sc_.p);
+               ticket_.p, sc_.p, (const double *)nullptr);
         else
             lk(4, k_cg_spmv<8, TM>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
-               ticket_.p, sc_.p);
+               ticket_.p, sc_.p, (const double *)nullptr);
     };
     if (icc) { sweep(true); sweep(false); }
     if (!zprev)
@@ -1295,13 +1319,15 @@ void Engine<D>::build_windows(bool fp32)
     win_valid_ = true;
 }
 
-// Mixed form: the ICCG on the FP32-stored matrix and factor (FP64 vectors
-// and arithmetic) with reliable updates.  Whenever the recursive residual
-// has fallen by kDelta since the last update, the true residual r = b - A x
+// Mixed form: the ICCG with the matrix and the IC(0) factor stored in FP32
+// (the SpMV in difference form, k_cg_spmv<.., true>) and FP64 vectors and
+// arithmetic, with reliable updates.  Whenever the recursive residual has
+// fallen by rel_delta_ since the last update, the true residual r = b - A x
 // is recomputed with the FP64 matrix and the iteration resumes from it with
 // its search direction kept.  Stops when ||b - A x|| <= max(cg_tolerance,
-// refine_tolerance * ||b||, kFloor * u * || |b| + |A| |x| ||) (u the FP64
-// unit roundoff), or when the true residual stalls.
+// refine_tolerance ||b||, kFloor u || |b| + |A| |x| ||), u the FP64 unit
+// roundoff: kFloor times the rounding floor of an FP64 residual, where the
+// FP64 form's own solve ends; or when the true residual stalls.
 template <int D>
 void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
 {
@@ -1334,16 +1360,23 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
     MPS_CUDA(cudaMemcpyAsync(sc_host_, sc_.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, st_));
     MPS_CUDA(cudaStreamSynchronize(st_));
     double bnorm = std::sqrt(sc_host_->rr_outer);
-    double rtol = prm_.refine_tolerance > 0.0 ? prm_.refine_tolerance : 1.0e-10;
-    double target = std::max(prm_.cg_tolerance, rtol * bnorm);
+    double target = std::max(prm_.cg_tolerance, std::max(prm_.refine_tolerance, 0.0) * bnorm);
     double rnorm = bnorm, rbest = bnorm, floor_norm = 0.0;
     int updates = 0, stalls = 0;
     PcgBufs<float> v{A32_.p,      xf32_lo_.p, xf32_up_.p, pkv32_lo_.p, pkv32_up_.p, dinv32_.p, inv32_cm_.p,
                      inv32_rm_.p, x_.p,       r_.p,       z_.p,        p_.p,        Ap_.p,     y_.p,
                      part_.p,     b_.p};
+    if (mixed_spmv_ == 1) v.A64 = A_.p;   // tuning alternatives of the inner SpMV
+    if (mixed_spmv_ == 2) {
+        dsum_.reserve((size_t)cap_);
+        launch(k_row_sum, nblk(n_eq, TPB), TPB, 0, st_, n_eq, (const int *)row_ptr_.p, (const double *)A_.p,
+               dsum_.p);
+        v.dsum = dsum_.p;
+    }
     const double *zsrc = icc ? z_.p : r_.p;   // the preconditioned residual
     if (rnorm > target) {
-        pcg_solve<float>(v, std::max(target, kDelta * rnorm), prm_.cg_max_iter, icc, n_eq, nnz);
+        pcg_solve<float>(v, std::max(target, rel_delta_ * rnorm), prm_.cg_max_iter, icc, n_eq, nnz);
+        double goal = target;
         for (;;) {
             MPS_CUDA(cudaMemcpyAsync(zprev_.p, zsrc, sizeof(double) * n_eq, cudaMemcpyDeviceToDevice, st_));
             launch(k_refine_residual, RB, CG_BLOCK, 0, st_, n_eq, (const int *)row_ptr_.p, (const int *)col_.p,
@@ -1358,10 +1391,13 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
             if (rnorm < kStall * rbest) stalls = 0;
             else stalls++;
             rbest = std::min(rbest, rnorm);
-            if (rnorm <= std::max(target, kFloor * floor_norm) || sc_host_->iter >= prm_.cg_max_iter ||
-                sc_host_->breakdown || updates >= kMaxUpdates || stalls >= kMaxStalls)
+            goal = std::max(target, kFloor * floor_norm);
+            if (rnorm <= goal || sc_host_->iter >= prm_.cg_max_iter || sc_host_->breakdown ||
+                updates >= kMaxUpdates || stalls >= kMaxStalls)
                 break;
-            pcg_solve<float>(v, std::max(target, kDelta * rnorm), prm_.cg_max_iter, icc, n_eq, nnz, zprev_.p);
+            // the next inner solve aims at most at the goal: its recursive
+            // residual tracks the true one closely (FP64 vectors)
+            pcg_solve<float>(v, std::max(goal, rel_delta_ * rnorm), prm_.cg_max_iter, icc, n_eq, nnz, zprev_.p);
         }
     }
     int inner = sc_host_->iter;

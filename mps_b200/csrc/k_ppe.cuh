@@ -918,10 +918,18 @@ constexpr int SPMV_U = 8;   // entries per lane loaded in one batch by the FP32 
 // Ap = A p and the p.Ap partial; the last block forms alpha.  The kernel
 // also performs the loop-head test of the reference (sqrt(r.r) < tol, and
 // the iteration cap) before any work.
-template <int LPR, class TM>
+//
+// DIFF (the mixed form's FP32 matrix): the product in difference form,
+// (A p)_i = dsum_i p_i + sum_j A_ij (p_j - p_i), dsum_i the FP64 row sum of A
+// (the diagonal entry contributes nothing to the second sum).  Rounding A_ij
+// to FP32 then perturbs the product in proportion to the differences of p
+// across a pair, not to |A_ij| |p_j|, whose cancellation in a Laplacian row
+// would amplify the rounding by orders of magnitude.
+template <int LPR, class TM, bool DIFF = false>
 __global__ void __launch_bounds__(CG_BLOCK, 8) k_cg_spmv(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ col,
                           const TM *__restrict__ A, const double *p, double *Ap,
-                          double *partials, unsigned *ticket, CGScalars *sc)
+                          double *partials, unsigned *ticket, CGScalars *sc,
+                          const double *__restrict__ dsum = nullptr)
 {
     using T = double;   // vectors and sums; TM is the storage type of the matrix
     __shared__ double sh[CG_BLOCK / 32];
@@ -958,16 +966,20 @@ __global__ void __launch_bounds__(CG_BLOCK, 8) k_cg_spmv(int n_eq, const int *__
                 a[u] = ok ? __ldg(&A[q]) : TM(0);
                 c[u] = ok ? __ldg(&col[q]) : -1;
             }
+            T pi = DIFF ? p[r] : T(0);
 #pragma unroll
             for (int u = 0; u < SPMV_U; u++)
-                if (c[u] >= 0) s += T(a[u]) * p[c[u]];
-            for (int q = q0 + SPMV_U * LPR; q < q1; q += LPR) s += T(__ldg(&A[q])) * p[__ldg(&col[q])];
+                if (c[u] >= 0) s += T(a[u]) * (DIFF ? p[c[u]] - pi : p[c[u]]);
+            for (int q = q0 + SPMV_U * LPR; q < q1; q += LPR)
+                s += T(__ldg(&A[q])) * (DIFF ? p[__ldg(&col[q])] - pi : p[__ldg(&col[q])]);
         }
 #pragma unroll
         for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LPR);
         if (lane == 0 && r < n_eq) {
+            double pr = p[r];
+            if (DIFF) s += __ldg(&dsum[r]) * pr;
             Ap[r] = s;
-            acc += p[r] * s;
+            acc += pr * s;
         }
     }
     double t = block_sum<CG_BLOCK>(acc, sh);
@@ -1091,6 +1103,17 @@ __global__ void k_convert(size_t n, const S *__restrict__ in, T *__restrict__ ou
 {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         out[i] = (T)in[i];
+}
+
+// dsum_i = sum_j A_ij in FP64, in entry order (the difference-form SpMV).
+__global__ void k_row_sum(int n_eq, const int *__restrict__ row_ptr, const double *__restrict__ A,
+                          double *__restrict__ dsum)
+{
+    int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_eq) return;
+    double s = 0.0;
+    for (int q = row_ptr[r]; q < row_ptr[r + 1]; q++) s += A[q];
+    dsum[r] = s;
 }
 
 // x = 0, r = b, ||b||^2 into sc->rr_outer.

@@ -17,7 +17,7 @@ from .types import HostParticles, particle_dtype
 
 class Session:
     def __init__(self, cfg, dim: int, capacity: int, precision: int = _lib.PREC_FP64,
-                 refine_tolerance: float = 1e-10, params: _lib.MpsParams | None = None):
+                 refine_tolerance: float = 0.0, params: _lib.MpsParams | None = None):
         self.lib = _lib.load()
         self.dim = dim
         self.cfg = cfg

@@ -343,8 +343,12 @@ def test_golden_trajectory_gpu():
 
 @pytest.mark.parametrize("steps", [1, 20])
 def test_mixed_precision_against_fp64(steps):
-    """The mixed form (FP32 inner ICCG + FP64 refinement) stays within the
-    1e-4 pressure relative-L2 target of the FP64 path, from the same state."""
+    """The mixed form (PPE matrix and IC(0) factor stored in FP32, FP64
+    vectors, reliable updates against the FP64 matrix) stays within the
+    1e-4 pressure relative-L2 target of the FP64 path, from the same state,
+    and ends its solve at the residual level the FP64 path reaches: the true
+    residual ||b - A x|| within 4x the FP64 rounding floor (or below the
+    1e-9 tolerance) and not above the FP64 path's own."""
     _cuda()
     from mps_b200 import _lib
     from mps_b200.session import start
@@ -357,13 +361,16 @@ def test_mixed_precision_against_fp64(steps):
     a.step(steps)
     b.step(steps)
     ga, gb = a.download(), b.download()
-    mb = b.metrics()
+    ma, mb = a.metrics(), b.metrics()
     a.close()
     b.close()
     assert np.array_equal(ga["type"], gb["type"])
     assert _rel(gb["pressure"], ga["pressure"]) < 1e-4
     assert _rel(gb["pos"], ga["pos"]) < 1e-6
     assert mb["ppe_outer"] >= 1 and mb["converged"] == 1
+    assert mb["ppe_true_residual"] <= max(cfg.cg_tolerance, 4.0 * mb["ppe_rounding_floor"])
+    assert mb["ppe_true_residual"] <= max(cfg.cg_tolerance, ma["ppe_true_residual"])
+    assert ma["ppe_true_residual"] > 0.0 and ma["ppe_rounding_floor"] > 0.0
 
 
 def test_set_precision_switches_the_form():
