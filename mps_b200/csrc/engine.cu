@@ -233,6 +233,16 @@ private:
     DevArray<int> inv_len_, inv_off_;        // in-cell block inverses: entries, offsets per active cell
     DevArray<double> inv_cm_, inv_rm_;       // column-major (forward) and row-major (backward) copies
     DevArray<int> colinv_, wfirst_;          // inverse offsets at colour boundaries; first cell per window
+    // jagged-diagonal cross blocks of the warp-per-cell sweep: diagonals per
+    // cell (jlen_, its scan jdc_*), diagonal slots (jdp_*), row of each rank
+    DevArray<int> jlen_, jdc_lo_, jdc_up_, jdp_lo_, jdp_up_;
+    DevArray<unsigned char> jperm_lo_, jperm_up_;
+    // sweep kernel (MPS_SWEEP): 1 the warp-per-cell k_sweep_cell (default), 0
+    // the windowed k_sweep_colour
+    int sweep_mode_ = 1;
+    // polls of the first wait for a staged block inverse (MPS_TEST_MBAR_POLLS
+    // lowers it, down to 0, to exercise the timeout path)
+    int first_polls_ = MBAR_POLLS;
     std::vector<int> nwin_, win_off_;        // windows per colour, their table offsets
 
 
@@ -368,6 +378,11 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
         if (v > 0.0 && v < 1.0) rel_delta_ = v;
     }
     if (const char *e = std::getenv("MPS_MIXED_SPMV")) mixed_spmv_ = std::atoi(e);
+    if (const char *e = std::getenv("MPS_SWEEP")) sweep_mode_ = std::atoi(e) == 0 ? 0 : 1;
+    if (const char *e = std::getenv("MPS_TEST_MBAR_POLLS")) {
+        int v = std::atoi(e);
+        if (v >= 0 && v < MBAR_POLLS) first_polls_ = v;
+    }
     if (const char *e = std::getenv("MPS_CELL_WIN")) {
         int v = std::atoi(e);
         if (v >= 256 && v <= CELL_WIN_MAX && v % 4 == 0) cell_win_ = v;
@@ -1094,14 +1109,41 @@ void Engine<D>::ppe(bool clamp)
             swc.thr_lo[k] = pf >= 0 ? row_off_[pf] : 0;
             swc.thr_up[k] = pb >= 0 ? row_off_[pb + 1] : 0x7fffffff;
         }
-        launch(k_cross_fill, nblk(n_eq, TPB), TPB, 0, st_, n_eq, (const int *)row_ptr_.p, (const int *)inpos_.p,
-               (const int *)outpos_.p, (const int *)col_.p, (const double *)F_.p, (const int *)xp_lo_.p,
-               (const int *)xp_up_.p, xc_lo_.p, xf_lo_.p, xc_up_.p, xf_up_.p, swc, xs_lo_.p, xs_up_.p);
         int nact = act_off_[ncol];
         adesc_.reserve((size_t)nact + 1);
         if (nact)
             launch(k_cell_desc, nblk(nact, TPB), TPB, 0, st_, nact, (const int *)acells_.p,
                    (const int *)cell_row0_.p, (const int *)ucount_.p, adesc_.p);
+        if (sweep_mode_ == 1) {
+            // the cross runs of each cell in jagged-diagonal order (k_sweep_cell)
+            for (auto *v : {&jlen_, &jdc_lo_, &jdc_up_}) v->reserve((size_t)nact + 1);
+            for (auto *v : {&jperm_lo_, &jperm_up_}) v->reserve((size_t)n_eq + 1);
+            for (int lo = 1; lo >= 0; lo--) {
+                DevArray<int> &jdc = lo ? jdc_lo_ : jdc_up_, &jdp = lo ? jdp_lo_ : jdp_up_;
+                const int *xp = lo ? xp_lo_.p : xp_up_.p;
+                if (nact)
+                    launch(k_jds_sizes, nblk((long long)nact * 32, 256), 256, 0, st_, nact, (const int2 *)adesc_.p,
+                           xp, jlen_.p, err_.p);
+                scan_exclusive<int>(jlen_.p, jdc.p, nact, scanws_.p, st_);
+                jdp.reserve((size_t)read_int(jdc.p + nact) + 1);
+                if (!nact) continue;
+                if (lo)
+                    launch(k_jds_fill<true>, nblk(nact, 4), 128, 0, st_, nact, (const int2 *)adesc_.p, xp,
+                           (const int *)jdc.p, (const int *)row_ptr_.p, (const int *)inpos_.p,
+                           (const int *)outpos_.p, (const int *)col_.p, (const double *)F_.p, jdp.p, jperm_lo_.p,
+                           xc_lo_.p, xf_lo_.p);
+                else
+                    launch(k_jds_fill<false>, nblk(nact, 4), 128, 0, st_, nact, (const int2 *)adesc_.p, xp,
+                           (const int *)jdc.p, (const int *)row_ptr_.p, (const int *)inpos_.p,
+                           (const int *)outpos_.p, (const int *)col_.p, (const double *)F_.p, jdp.p, jperm_up_.p,
+                           xc_up_.p, xf_up_.p);
+            }
+        } else {
+            launch(k_cross_fill, nblk(n_eq, TPB), TPB, 0, st_, n_eq, (const int *)row_ptr_.p,
+                   (const int *)inpos_.p, (const int *)outpos_.p, (const int *)col_.p, (const double *)F_.p,
+                   (const int *)xp_lo_.p, (const int *)xp_up_.p, xc_lo_.p, xf_lo_.p, xc_up_.p, xf_up_.p, swc,
+                   xs_lo_.p, xs_up_.p);
+        }
         // inverses of the in-cell diagonal blocks of the factor, and the
         // windows of each colour's range for the staged in-cell sweeps
         inv_len_.reserve((size_t)nact + 1);
@@ -1126,7 +1168,7 @@ void Engine<D>::ppe(bool clamp)
                    (const double *)pk_val_lo_.p, (const unsigned char *)pk_k_lo_.p, (const double *)dinv_.p,
                    inv_cm_.p, inv_rm_.p);
         win_valid_ = false;
-        build_windows(prm_.precision == MPS_PREC_MIXED);
+        if (sweep_mode_ == 0) build_windows(prm_.precision == MPS_PREC_MIXED);
         met.sweep_cross_lo = nx_lo_;
         met.sweep_cross_up = nx_up_;
         met.sweep_inverse_entries = ninv_;
@@ -1202,6 +1244,20 @@ void Engine<D>::pcg_solve(const PcgBufs<TM> &v, double tol, int maxit, bool icc,
         for (int i = 0; i < ncol; i++) {
             int c = fwdir ? i : ncol - 1 - i;
             if (act_off_[c + 1] > act_off_[c]) order[nc++] = c;
+        }
+        if (sweep_mode_ == 1) {
+            auto cellk = fwdir ? k_sweep_cell<true, TM> : k_sweep_cell<false, TM>;
+            for (int i = 0; i < nc; i++) {
+                int c = order[i];
+                int kb = act_off_[c], ke = act_off_[c + 1];
+                lk(2, cellk, nblk(ke - kb, JW), 32 * JW, 0, kb, ke, (const int2 *)adesc_.p, (const int *)inv_off_.p,
+                   fwdir ? v.inv_cm : v.inv_rm, pko, pkl, pkv, pkk, v.dinv, (const int *)(fwdir ? xp_lo_.p : xp_up_.p),
+                   (const int *)(fwdir ? jdc_lo_.p : jdc_up_.p), (const int *)(fwdir ? jdp_lo_.p : jdp_up_.p),
+                   (const unsigned char *)(fwdir ? jperm_lo_.p : jperm_up_.p),
+                   (const int *)(fwdir ? xc_lo_.p : xc_up_.p), fwdir ? v.xf_lo : v.xf_up, (const T *)rhs, out,
+                   (const CGScalars *)sc_.p, first_polls_, err_.p);
+            }
+            return;
         }
         auto colk = fwdir ? k_sweep_colour<true, TM> : k_sweep_colour<false, TM>;
         for (int i = 0; i < nc; i++) {
@@ -1646,7 +1702,7 @@ void Engine<D>::step_adjoint()
             PcgBufs<double> v{A_.p,      xf_lo_.p, xf_up_.p, pk_val_lo_.p, pk_val_up_.p, dinv_.p, inv_cm_.p,
                               inv_rm_.p, x_.p,     r_.p,     z_.p,         p_.p,         Ap_.p,   y_.p,
                               part_.p,   b_.p};
-            if (icc) build_windows(false);   // FP64 sweeps: FP64 windows
+            if (icc && sweep_mode_ == 0) build_windows(false);   // FP64 sweeps: FP64 windows
             pcg_solve<double>(v, kAdjRtol, prm_.cg_max_iter, icc, n_eq, nnz_);
             launch(k_adj_mu, RB, CG_BLOCK, 0, st_, n_eq, (const int *)part_of_row_.p, (const int *)S().id,
                    (const double *)x_.p, bnorm, adj_.mu);

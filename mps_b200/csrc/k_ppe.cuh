@@ -894,6 +894,233 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
     }
 }
 
+// ---- warp-per-cell sweep over jagged-diagonal cross runs ----------------------
+//
+// k_sweep_cell does colour c's whole part of a sweep in one launch, a warp
+// per cell: the cross-cell products of the cell's rows from colours swept
+// before c, then the in-cell product with the cell's block inverse.
+//
+// The cross entries of a cell's rows are stored cell by cell in
+// jagged-diagonal order (built once per step by k_jds_fill): the rows are
+// ranked by their number of cross entries, longest first, and entry k of the
+// row of rank q sits at jdp[k] + q, jdp[k] = first slot of the cell's k-th
+// diagonal.  A warp reads a diagonal with consecutive lanes on consecutive
+// addresses, every row's sum runs in its own entry order in one lane, and no
+// padding is stored (diagonal k holds only the rows that have a k-th entry).
+// The cell's block inverse is staged in shared memory by one bulk copy per
+// warp, issued with the other loads before pdl_wait().
+
+constexpr int JW = 4;                 // warps (cells in flight) per CTA
+constexpr int JSTAGE_M = 40;          // cells of up to this many unknowns stage their block inverse
+constexpr int JSTAGE = ((JSTAGE_M * (JSTAGE_M + 1) / 2) + 3) & ~3;
+constexpr int JU = 8;                 // cross entries per lane and row loaded in one batch
+constexpr int JMAXL = 512;            // cross entries of one row, at most (the list's max_neighbors bound)
+constexpr int MBAR_DRAIN_POLLS = 1 << 26;
+
+// Diagonals of every active cell's jagged-diagonal block: 1 + the longest
+// cross run among its rows (xp: the runs' offsets in row order).
+__global__ void k_jds_sizes(int nact, const int2 *__restrict__ desc, const int *__restrict__ xp,
+                            int *__restrict__ jlen, unsigned *err)
+{
+    int kk = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    int lane = threadIdx.x & 31;
+    if (kk >= nact) return;   // warp-uniform
+    int2 dd = desc[kk];
+    int lmax = 0;
+    for (int i = lane; i < dd.y; i += 32) lmax = max(lmax, xp[dd.x + i + 1] - xp[dd.x + i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lmax = max(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    if (lane == 0) {
+        if (lmax > JMAXL || dd.y > 255) atomicOr(err, ERR_CELL_OVERFULL);
+        jlen[kk] = min(lmax, JMAXL) + 1;
+    }
+}
+
+// Jagged-diagonal block of every active cell (a warp per cell, 4 per CTA):
+// ranks (longest run first, ties by row), jperm[r0 + rank] = row within the
+// cell, jdp[jdc[kk] + k] = slot of diagonal k (k = 0 .. longest; the last is
+// the block's end), and the entries: lo (forward) the lower cross run
+// [row_ptr, inpos) of each row, up (backward) the upper one [outpos,
+// row_ptr + 1).  The block occupies the same slots [xp[r0], xp[r0 + m]) as
+// the runs in row order.
+template <bool LO>
+__global__ void __launch_bounds__(128)
+k_jds_fill(int nact, const int2 *__restrict__ desc, const int *__restrict__ xp, const int *__restrict__ jdc,
+           const int *__restrict__ row_ptr, const int *__restrict__ inpos, const int *__restrict__ outpos,
+           const int *__restrict__ col, const double *__restrict__ F, int *__restrict__ jdp,
+           unsigned char *__restrict__ jperm, int *__restrict__ xc, double *__restrict__ xf)
+{
+    __shared__ int slen[4][256];
+    __shared__ int sjd[4][JMAXL + 1];
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int kk = blockIdx.x * 4 + w;
+    if (kk >= nact) return;   // warp-uniform; no block barrier below
+    int2 dd = desc[kk];
+    int r0 = dd.x, m = min(dd.y, 255);
+    int j0 = jdc[kk], nk = jdc[kk + 1] - j0 - 1;
+    int base = xp[r0];
+    for (int i = lane; i < m; i += 32) slen[w][i] = min(xp[r0 + i + 1] - xp[r0 + i], JMAXL);
+    __syncwarp();
+    // diagonal k holds the rows longer than k; its slot is the sum of the
+    // earlier diagonals' sizes
+    int carry = 0;
+    for (int k0 = 0; k0 <= nk; k0 += 32) {
+        int k = k0 + lane;
+        int cnt = 0;
+        if (k < nk)
+            for (int i = 0; i < m; i++) cnt += slen[w][i] > k;
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (k <= nk) sjd[w][k] = base + carry + incl - cnt;
+        carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+    __syncwarp();
+    for (int k = lane; k <= nk; k += 32) jdp[j0 + k] = sjd[w][k];
+    for (int i = lane; i < m; i += 32) {
+        int li = slen[w][i];
+        int rank = 0;
+        for (int j = 0; j < m; j++) {
+            int lj = slen[w][j];
+            rank += (lj > li) || (lj == li && j < i);
+        }
+        jperm[r0 + rank] = (unsigned char)i;
+        int r = r0 + i;
+        int src = LO ? row_ptr[r] : outpos[r];
+        for (int k = 0; k < li; k++) {
+            int dst = sjd[w][k] + rank;
+            xc[dst] = col[src + k];
+            xf[dst] = F[src + k];
+        }
+    }
+}
+
+// Bounded wait for a warp's bulk copy: false (and ERR_COPY_TIMEOUT set)
+// after `polls` polls, in which case the copy is first waited for with the
+// long bound, so that the warp never leaves it in flight.
+__device__ __forceinline__ bool stage_wait(unsigned bar, int polls, unsigned *err)
+{
+    if (mbar_wait(bar, 0, polls)) return true;
+    atomicOr(err, ERR_COPY_TIMEOUT);
+    for (int i = 0; i < MBAR_DRAIN_POLLS; i++) {
+        if (mbar_wait(bar, 0, 1)) break;
+        __nanosleep(64);
+    }
+    return false;
+}
+
+template <bool FWD, class TM>
+__global__ void __launch_bounds__(32 * JW)
+k_sweep_cell(int kbeg, int kend, const int2 *__restrict__ desc, const int *__restrict__ inv_off,
+             const TM *__restrict__ inv, const int *__restrict__ pk_off, const int *__restrict__ pk_len,
+             const TM *__restrict__ pk_val, const unsigned char *__restrict__ pk_k, const TM *__restrict__ dinv,
+             const int *__restrict__ xp, const int *__restrict__ jdc, const int *__restrict__ jdp,
+             const unsigned char *__restrict__ jperm, const int *__restrict__ xc, const TM *__restrict__ xf,
+             const double *rhs, double *x, const CGScalars *sc, int first_polls, unsigned *err)
+{
+    using T = double;   // vectors and sums; TM is the storage type of the factor
+    __shared__ __align__(128) TM stage[JW][JSTAGE];
+    __shared__ T spart[JW][SWEEP_MAXM];
+    __shared__ __align__(8) unsigned long long bars[JW];
+    pdl_trigger();
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int kk = kbeg + blockIdx.x * JW + w;
+    if (kk >= kend) {   // warp-uniform; no block barrier in this kernel
+        pdl_wait();
+        return;
+    }
+    int2 dd = __ldg(&desc[kk]);
+    int r0 = dd.x, m = dd.y;
+    int io = __ldg(&inv_off[kk]);
+    int nb = __ldg(&inv_off[kk + 1]) - io;
+    bool staged = m <= JSTAGE_M && nb > 0;
+    unsigned bar = smem_u32(&bars[w]);
+    if (staged && lane == 0) {
+        mbar_init(bar, 1);
+        mbar_arrive_expect_tx(bar, (unsigned)nb * (unsigned)sizeof(TM));
+        bulk_g2s(smem_u32(stage[w]), inv + io, (unsigned)nb * (unsigned)sizeof(TM), bar);
+    }
+    int jb = __ldg(&jdc[kk]);
+    // the first batch of the lane's first row (rank = lane): factor values
+    // and columns are written once per step, before the CG loop
+    int i0 = 0, len0 = 0;
+    TM f[JU];
+    int c[JU];
+    if (lane < m) {
+        i0 = __ldg(&jperm[r0 + lane]);
+        len0 = __ldg(&xp[r0 + i0 + 1]) - __ldg(&xp[r0 + i0]);
+    }
+#pragma unroll
+    for (int u = 0; u < JU; u++) {
+        bool ok = u < len0;
+        int q = ok ? __ldg(&jdp[jb + u]) + lane : 0;
+        f[u] = ok ? __ldg(&xf[q]) : TM(0);
+        c[u] = ok ? __ldg(&xc[q]) : -1;
+    }
+    pdl_wait();
+    if (sc->done) {
+        if (staged) stage_wait(bar, MBAR_DRAIN_POLLS, err);
+        return;
+    }
+    const bool big = m > SWEEP_MAXM;   // substitution in place in x (only in a blow-up)
+    for (int q0 = lane; q0 < m; q0 += 32) {
+        int i = q0 == lane ? i0 : __ldg(&jperm[r0 + q0]);
+        int len = q0 == lane ? len0 : __ldg(&xp[r0 + i + 1]) - __ldg(&xp[r0 + i]);
+        T s = T(0);
+        for (int k0 = 0; k0 < len; k0 += JU) {
+            if (k0 > 0 || q0 != lane) {
+#pragma unroll
+                for (int u = 0; u < JU; u++) {
+                    bool ok = k0 + u < len;
+                    int q = ok ? __ldg(&jdp[jb + k0 + u]) + q0 : 0;
+                    f[u] = ok ? __ldg(&xf[q]) : TM(0);
+                    c[u] = ok ? __ldg(&xc[q]) : -1;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < JU; u++)
+                if (c[u] >= 0) s += T(f[u]) * x[c[u]];
+        }
+        T pv = rhs[r0 + i] - s;
+        if (big) x[r0 + i] = pv;
+        else spart[w][i] = pv;
+    }
+    if (big) {
+        __threadfence_block();
+        __syncwarp();
+        for (int t = 0; t < m; t++) {
+            int r = FWD ? r0 + t : r0 + m - 1 - t;
+            int po = pk_off[r], l = pk_len[r];
+            T ps = T(0);
+            for (int e = lane; e < l; e += 32) ps += T(pk_val[po + e]) * x[r0 + pk_k[po + e]];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, o);
+            if (lane == 0) x[r] = (x[r] - ps) * T(dinv[r]);
+            __threadfence_block();
+            __syncwarp();
+        }
+        return;
+    }
+    __syncwarp();
+    const TM *blk = inv + io;
+    if (staged) {
+        if (!stage_wait(bar, first_polls, err)) return;
+        blk = stage[w];
+    }
+    for (int i = lane; i < m; i += 32) {
+        T y = T(0);
+        if (FWD) {
+            for (int j = 0; j <= i; j++) y += T(blk[tri_colofs(j, m) + i - j]) * spart[w][j];
+        } else {
+            for (int j = i; j < m; j++) y += T(blk[j * (j + 1) / 2 + i]) * spart[w][j];
+        }
+        x[r0 + i] = y;
+    }
+}
+
 // ---- CG vector kernels ------------------------------------------------------
 //
 // The kernels of one CG iteration (SpMV, axpy, the sweeps, r.z, p update) are
