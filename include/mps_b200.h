@@ -204,6 +204,30 @@ int  mps_get_cell_links(mps_session *s, int *head, int *next, int total_cells);
 int  mps_get_ppe(mps_session *s, int *eq_idx, int *row_ptr, int *col_idx, double *val,
                  double *b, int *n_eq, long long *nnz);
 
+/* The last step's PPE and IC(0) preconditioner in the solver's own unknown
+ * numbering (block colour order: colour by colour, cell by cell), for
+ * checking the factorisation (pressure_solver.c:156-232 restated on this
+ * ordering) and the sweeps.  ICCG sessions only.
+ *
+ * mps_get_ic0: row_ptr[n_eq+1], col[nnz] (sorted), A[nnz] and b[n_eq] (FP64)
+ * and F[nnz], the factor in A's pattern: L_ij below the diagonal, 1/L_ii on
+ * it, L_ji above it.  row_ptr == NULL returns the sizes only; other NULL
+ * pointers are skipped.
+ * mps_get_cell_blocks: per active cell k in colour order cells[2k] = first
+ * row, cells[2k+1] = unknowns m; inv_off[ncells+1]; inv[ninv] the inverse of
+ * each cell's diagonal block of L (FP64) at inv_off[k], column-major over
+ * the lower triangle: (L_cc^-1)_ij (i >= j) at j*m - j*(j-1)/2 + (i - j)
+ * (0 entries for cells above 64 unknowns, which the sweeps solve by
+ * substitution); colour_rows[2^dim + 1] the first row of each colour.
+ * mps_apply_preconditioner: z = (L L^T)^-1 r by the device sweeps of the
+ * last solve's form (the FP32 factor copies after a mixed-form solve); r, z
+ * are host arrays of n_eq doubles in the solver's numbering. */
+int  mps_get_ic0(mps_session *s, int *row_ptr, int *col, double *A, double *F, double *b, int *n_eq,
+                 long long *nnz);
+int  mps_get_cell_blocks(mps_session *s, int *cells, int *inv_off, double *inv, int *colour_rows, int *ncells,
+                         long long *ninv);
+int  mps_apply_preconditioner(mps_session *s, const double *r, double *z);
+
 int  mps_get_metrics(mps_session *s, mps_metrics_t *m);
 
 /* Kernels launched by this library in this process so far. */

@@ -147,6 +147,9 @@ SIGNATURES = {
     "mps_get_cell_index": (I, [P, P]),
     "mps_get_cell_links": (I, [P, P, P, I]),
     "mps_get_ppe": (I, [P, P, P, P, P, P, IP, C.POINTER(C.c_longlong)]),
+    "mps_get_ic0": (I, [P, P, P, P, P, P, IP, C.POINTER(C.c_longlong)]),
+    "mps_get_cell_blocks": (I, [P, P, P, P, P, IP, C.POINTER(C.c_longlong)]),
+    "mps_apply_preconditioner": (I, [P, P, P]),
     "mps_get_metrics": (I, [P, C.POINTER(MpsMetrics)]),
     "mps_get_stream": (P, [P]),
     "mps_launch_count": (C.c_ulonglong, []),

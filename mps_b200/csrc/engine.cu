@@ -185,6 +185,10 @@ public:
     void get_ppe(int *eq_idx, int *row_ptr, int *col, double *val, double *b, int *n_eq,
                  long long *nnz) override;
     void run_stage(int stage, const int *nb, const int *cnt, int max_nb, double arg) override;
+    void get_ic0(int *row_ptr, int *col, double *A, double *F, double *b, int *n_eq, long long *nnz) override;
+    void get_cell_blocks(int *cells, int *inv_off, double *inv, int *colour_rows, int *ncells,
+                         long long *ninv) override;
+    void apply_preconditioner(const double *r, double *z) override;
     cudaStream_t stream() const override { return st_; }
     size_t state_bytes() const override;
     void state_save(void *dst) override;
@@ -237,12 +241,16 @@ private:
     // cell (jlen_, its scan jdc_*), diagonal slots (jdp_*), row of each rank
     DevArray<int> jlen_, jdc_lo_, jdc_up_, jdp_lo_, jdp_up_;
     DevArray<unsigned char> jperm_lo_, jperm_up_;
-    // sweep kernel (MPS_SWEEP): 1 the warp-per-cell k_sweep_cell (default), 0
-    // the windowed k_sweep_colour
-    int sweep_mode_ = 1;
+    // sweep kernel (MPS_SWEEP): 0 the windowed k_sweep_colour (default), 1
+    // the CTA-per-cell k_sweep_cell over jagged-diagonal cross blocks
+    int sweep_mode_ = 0;
     // polls of the first wait for a staged block inverse (MPS_TEST_MBAR_POLLS
     // lowers it, down to 0, to exercise the timeout path)
     int first_polls_ = MBAR_POLLS;
+    // k_sweep_cell lets its dependent launch start at its beginning (1) or
+    // only as its CTAs exit (0); MPS_CELL_EARLY overrides
+    int cell_early_ = 0;
+    int num_sms_ = 148;
     std::vector<int> nwin_, win_off_;        // windows per colour, their table offsets
 
 
@@ -276,6 +284,8 @@ private:
     bool win_valid_ = false;               // the window tables match the current factor and win_
     std::vector<int> inv_col_off_;         // block-inverse offsets at the colour boundaries
     bool ppe_valid_ = false;
+    bool ic0_valid_ = false;     // the IC(0) factor and its sweep tables belong to the last PPE
+    bool last_fp32_ = false;     // the last solve ran the mixed form (FP32 factor copies exist)
 
     // ---- driven walls
     long long tstep_ = 0;                    // steps taken since the last upload (time = tstep_ dt)
@@ -336,6 +346,8 @@ private:
     template <class TM>
     void pcg_solve(const PcgBufs<TM> &v, double tol, int maxit, bool icc, int n_eq, long long nnz,
                    const double *zprev = nullptr);
+    template <class TM>
+    void run_sweep(const PcgBufs<TM> &v, bool fwdir);
     void mixed_solve(int n_eq, long long nnz, bool icc);
     void build_windows(bool fp32);
     static constexpr int kMaxUpdates = 200;      // reliable updates of the mixed form, at most
@@ -378,7 +390,13 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
         if (v > 0.0 && v < 1.0) rel_delta_ = v;
     }
     if (const char *e = std::getenv("MPS_MIXED_SPMV")) mixed_spmv_ = std::atoi(e);
-    if (const char *e = std::getenv("MPS_SWEEP")) sweep_mode_ = std::atoi(e) == 0 ? 0 : 1;
+    if (const char *e = std::getenv("MPS_SWEEP")) sweep_mode_ = std::atoi(e) == 1 ? 1 : 0;
+    if (const char *e = std::getenv("MPS_CELL_EARLY")) cell_early_ = std::atoi(e) != 0;
+    {
+        int dev = 0;
+        MPS_CUDA(cudaGetDevice(&dev));
+        MPS_CUDA(cudaDeviceGetAttribute(&num_sms_, cudaDevAttrMultiProcessorCount, dev));
+    }
     if (const char *e = std::getenv("MPS_TEST_MBAR_POLLS")) {
         int v = std::atoi(e);
         if (v >= 0 && v < MBAR_POLLS) first_polls_ = v;
@@ -1175,6 +1193,8 @@ void Engine<D>::ppe(bool clamp)
     }
     MPS_CUDA(cudaEventRecord(ev_[3], st_));
 
+    ic0_valid_ = icc;
+    last_fp32_ = prm_.precision == MPS_PREC_MIXED;
     if (prm_.precision == MPS_PREC_MIXED) {
         mixed_solve(n_eq, nnz, icc);
     } else {
@@ -1198,6 +1218,65 @@ void Engine<D>::ppe(bool clamp)
     launch(k_writeback<D>, nb, TPB, 0, st_, s, row_of_.p, x_.p, n, clamp);
     MPS_CUDA(cudaGetLastError());
     ppe_valid_ = true;
+}
+
+// One IC(0) sweep of the current factor, forward (rhs v.r, result v.y) or
+// backward (rhs v.y, result v.z), colour by colour: the cross-cell products
+// of each colour's rows from the colours swept before it, then the in-cell
+// products with the block inverses.
+template <int D>
+template <class TM>
+void Engine<D>::run_sweep(const PcgBufs<TM> &v, bool fwdir)
+{
+    using T = double;
+    int ncol = 1 << D;
+    auto lk = [&](int bit, auto kern, dim3 g, dim3 b, size_t sm, auto... args) {
+        if (pdl_mask_ & bit) launch_pdl(kern, g, b, sm, st_, args...);
+        else launch(kern, g, b, sm, st_, args...);
+    };
+    {
+        const T *rhs = fwdir ? v.r : v.y;
+        T *out = fwdir ? v.y : v.z;
+        const int *pko = fwdir ? pk_off_lo_.p : pk_off_up_.p, *pkl = fwdir ? pk_len_lo_.p : pk_len_up_.p;
+        const TM *pkv = fwdir ? v.pkv_lo : v.pkv_up;
+        const unsigned char *pkk = fwdir ? pk_k_lo_.p : pk_k_up_.p;
+        int order[8], nc = 0;
+        for (int i = 0; i < ncol; i++) {
+            int c = fwdir ? i : ncol - 1 - i;
+            if (act_off_[c + 1] > act_off_[c]) order[nc++] = c;
+        }
+        if (sweep_mode_ == 1) {
+            auto cellk = fwdir ? k_sweep_cell<true, TM> : k_sweep_cell<false, TM>;
+            int resident = 0;
+            MPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, cellk, 32 * JW, 0));
+            resident *= num_sms_;
+            for (int i = 0; i < nc; i++) {
+                int c = order[i];
+                int kb = act_off_[c], ke = act_off_[c + 1];
+                // the last wave's CTAs trigger the next launch (cell_early_: all of them)
+                int from = cell_early_ ? 0 : std::max(0, ke - kb - resident);
+                lk(2, cellk, ke - kb, 32 * JW, 0, kb, ke, (const int2 *)adesc_.p, (const int *)inv_off_.p,
+                   fwdir ? v.inv_cm : v.inv_rm, pko, pkl, pkv, pkk, v.dinv,
+                   (const int *)(fwdir ? jdc_lo_.p : jdc_up_.p), (const int *)(fwdir ? jdp_lo_.p : jdp_up_.p),
+                   (const unsigned char *)(fwdir ? jperm_lo_.p : jperm_up_.p),
+                   (const int *)(fwdir ? xc_lo_.p : xc_up_.p), fwdir ? v.xf_lo : v.xf_up, (const T *)rhs, out,
+                   (const CGScalars *)sc_.p, first_polls_, from, err_.p);
+            }
+            return;
+        }
+        auto colk = fwdir ? k_sweep_colour<true, TM> : k_sweep_colour<false, TM>;
+        for (int i = 0; i < nc; i++) {
+            int c = order[i], cn = i + 1 < nc ? order[i + 1] : -1;
+            int nrb = cn >= 0 ? row_off_[cn] : 0, nre = cn >= 0 ? row_off_[cn + 1] : 0;
+            int ncb = cn >= 0 ? nblk((long long)(nre - nrb) * 8, CELL_THREADS) : 0;
+            lk(2, colk, nwin_[c] + ncb, CELL_THREADS, sizeof(TM) * (win_ + CELL_MAXBLK),
+               (const int *)wfirst_.p + win_off_[c], nwin_[c], (const int2 *)adesc_.p, (const int *)inv_off_.p,
+               fwdir ? v.inv_cm : v.inv_rm, pko, pkl, pkv, pkk, v.dinv, (const int *)(fwdir ? xp_lo_.p : xp_up_.p),
+               (const int *)(fwdir ? xs_lo_.p : xs_up_.p), (const int *)(fwdir ? xc_lo_.p : xc_up_.p),
+               fwdir ? v.xf_lo : v.xf_up, (int)(i == 0), nrb, nre, rhs, v.part, out, (const CGScalars *)sc_.p,
+               win_ + CELL_MAXBLK, err_.p);
+        }
+    }
 }
 
 // PCG of pressure_solver.c:261-322 (CG of :90-131 when icc is false) on the
@@ -1231,47 +1310,7 @@ void Engine<D>::pcg_solve(const PcgBufs<TM> &v, double tol, int maxit, bool icc,
         if (pdl_mask_ & bit) launch_pdl(kern, g, b, sm, st_, args...);
         else launch(kern, g, b, sm, st_, args...);
     };
-    // IC(0) sweeps per colour: the cross-cell products of all the colour's
-    // rows, then the in-cell product a warp per cell from the staged block
-    // inverses.
-    auto sweep = [&](bool fwdir) {
-        const T *rhs = fwdir ? v.r : v.y;
-        T *out = fwdir ? v.y : v.z;
-        const int *pko = fwdir ? pk_off_lo_.p : pk_off_up_.p, *pkl = fwdir ? pk_len_lo_.p : pk_len_up_.p;
-        const TM *pkv = fwdir ? v.pkv_lo : v.pkv_up;
-        const unsigned char *pkk = fwdir ? pk_k_lo_.p : pk_k_up_.p;
-        int order[8], nc = 0;
-        for (int i = 0; i < ncol; i++) {
-            int c = fwdir ? i : ncol - 1 - i;
-            if (act_off_[c + 1] > act_off_[c]) order[nc++] = c;
-        }
-        if (sweep_mode_ == 1) {
-            auto cellk = fwdir ? k_sweep_cell<true, TM> : k_sweep_cell<false, TM>;
-            for (int i = 0; i < nc; i++) {
-                int c = order[i];
-                int kb = act_off_[c], ke = act_off_[c + 1];
-                lk(2, cellk, nblk(ke - kb, JW), 32 * JW, 0, kb, ke, (const int2 *)adesc_.p, (const int *)inv_off_.p,
-                   fwdir ? v.inv_cm : v.inv_rm, pko, pkl, pkv, pkk, v.dinv, (const int *)(fwdir ? xp_lo_.p : xp_up_.p),
-                   (const int *)(fwdir ? jdc_lo_.p : jdc_up_.p), (const int *)(fwdir ? jdp_lo_.p : jdp_up_.p),
-                   (const unsigned char *)(fwdir ? jperm_lo_.p : jperm_up_.p),
-                   (const int *)(fwdir ? xc_lo_.p : xc_up_.p), fwdir ? v.xf_lo : v.xf_up, (const T *)rhs, out,
-                   (const CGScalars *)sc_.p, first_polls_, err_.p);
-            }
-            return;
-        }
-        auto colk = fwdir ? k_sweep_colour<true, TM> : k_sweep_colour<false, TM>;
-        for (int i = 0; i < nc; i++) {
-            int c = order[i], cn = i + 1 < nc ? order[i + 1] : -1;
-            int nrb = cn >= 0 ? row_off_[cn] : 0, nre = cn >= 0 ? row_off_[cn + 1] : 0;
-            int ncb = cn >= 0 ? nblk((long long)(nre - nrb) * 8, CELL_THREADS) : 0;
-            lk(2, colk, nwin_[c] + ncb, CELL_THREADS, sizeof(TM) * (win_ + CELL_MAXBLK),
-               (const int *)wfirst_.p + win_off_[c], nwin_[c], (const int2 *)adesc_.p, (const int *)inv_off_.p,
-               fwdir ? v.inv_cm : v.inv_rm, pko, pkl, pkv, pkk, v.dinv, (const int *)(fwdir ? xp_lo_.p : xp_up_.p),
-               (const int *)(fwdir ? xs_lo_.p : xs_up_.p), (const int *)(fwdir ? xc_lo_.p : xc_up_.p),
-               fwdir ? v.xf_lo : v.xf_up, (int)(i == 0), nrb, nre, rhs, v.part, out, (const CGScalars *)sc_.p,
-               win_ + CELL_MAXBLK, err_.p);
-        }
-    };
+    auto sweep = [&](bool fwdir) { run_sweep<TM>(v, fwdir); };
     const int lpr = spmv_lpr_ ? spmv_lpr_ : (sizeof(TM) == 8 ? 8 : 16);
     auto spmv = [&]() {
         const int *rp = row_ptr_.p, *ci = col_.p;
@@ -1877,6 +1916,68 @@ void Engine<D>::get_ppe(int *eq_idx, int *row_ptr, int *col, double *val, double
     if (eq_idx) std::memcpy(eq_idx, h_eq.data(), sizeof(int) * n);
 }
 
+template <int D>
+void Engine<D>::get_ic0(int *row_ptr, int *col, double *A, double *F, double *b, int *n_eq, long long *nnz)
+{
+    if (!ppe_valid_ || !ic0_valid_) throw CudaError("no IC(0) factor: run an ICCG step first", MPS_ERR_INVALID);
+    if (n_eq) *n_eq = n_eq_;
+    if (nnz) *nnz = nnz_;
+    if (!row_ptr) return;
+    int ne = n_eq_;
+    MPS_CUDA(cudaMemcpyAsync(row_ptr, row_ptr_.p, sizeof(int) * (ne + 1), cudaMemcpyDeviceToHost, st_));
+    if (col) MPS_CUDA(cudaMemcpyAsync(col, col_.p, sizeof(int) * nnz_, cudaMemcpyDeviceToHost, st_));
+    if (A) MPS_CUDA(cudaMemcpyAsync(A, A_.p, sizeof(double) * nnz_, cudaMemcpyDeviceToHost, st_));
+    if (F) MPS_CUDA(cudaMemcpyAsync(F, F_.p, sizeof(double) * nnz_, cudaMemcpyDeviceToHost, st_));
+    if (b) MPS_CUDA(cudaMemcpyAsync(b, b_.p, sizeof(double) * ne, cudaMemcpyDeviceToHost, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+}
+
+template <int D>
+void Engine<D>::get_cell_blocks(int *cells, int *inv_off, double *inv, int *colour_rows, int *ncells,
+                                long long *ninv)
+{
+    if (!ppe_valid_ || !ic0_valid_) throw CudaError("no IC(0) factor: run an ICCG step first", MPS_ERR_INVALID);
+    int ncol = 1 << D;
+    int nact = act_off_[ncol];
+    if (ncells) *ncells = nact;
+    if (ninv) *ninv = ninv_;
+    if (colour_rows)
+        for (int c = 0; c <= ncol; c++) colour_rows[c] = row_off_[c];
+    if (cells && nact) MPS_CUDA(cudaMemcpyAsync(cells, adesc_.p, sizeof(int2) * nact, cudaMemcpyDeviceToHost, st_));
+    if (inv_off) MPS_CUDA(cudaMemcpyAsync(inv_off, inv_off_.p, sizeof(int) * (nact + 1), cudaMemcpyDeviceToHost, st_));
+    if (inv && ninv_) MPS_CUDA(cudaMemcpyAsync(inv, inv_cm_.p, sizeof(double) * ninv_, cudaMemcpyDeviceToHost, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+}
+
+template <int D>
+void Engine<D>::apply_preconditioner(const double *r, double *z)
+{
+    if (!ppe_valid_ || !ic0_valid_) throw CudaError("no IC(0) factor: run an ICCG step first", MPS_ERR_INVALID);
+    if (!r || !z) throw CudaError("null vector", MPS_ERR_INVALID);
+    int ne = n_eq_;
+    MPS_CUDA(cudaMemcpyAsync(r_.p, r, sizeof(double) * ne, cudaMemcpyHostToDevice, st_));
+    MPS_CUDA(cudaMemsetAsync(&sc_.p->done, 0, sizeof(int), st_));
+    if (last_fp32_) {
+        if (sweep_mode_ == 0) build_windows(true);
+        PcgBufs<float> v{A32_.p,      xf32_lo_.p, xf32_up_.p, pkv32_lo_.p, pkv32_up_.p, dinv32_.p, inv32_cm_.p,
+                         inv32_rm_.p, x_.p,       r_.p,       z_.p,        p_.p,        Ap_.p,     y_.p,
+                         part_.p,     b_.p};
+        run_sweep<float>(v, true);
+        run_sweep<float>(v, false);
+    } else {
+        if (sweep_mode_ == 0) build_windows(false);
+        PcgBufs<double> v{A_.p,      xf_lo_.p, xf_up_.p, pk_val_lo_.p, pk_val_up_.p, dinv_.p, inv_cm_.p,
+                          inv_rm_.p, x_.p,     r_.p,     z_.p,         p_.p,         Ap_.p,   y_.p,
+                          part_.p,   b_.p};
+        run_sweep<double>(v, true);
+        run_sweep<double>(v, false);
+    }
+    MPS_CUDA(cudaGetLastError());
+    MPS_CUDA(cudaMemcpyAsync(z, z_.p, sizeof(double) * ne, cudaMemcpyDeviceToHost, st_));
+    MPS_CUDA(cudaStreamSynchronize(st_));
+    check_err();
+}
+
 // ---- stages over a caller list (drop-in fine-grained functions) ----------------
 
 template <int D>
@@ -2110,6 +2211,23 @@ int mps_get_ppe(mps_session *s, int *eq_idx, int *row_ptr, int *col_idx, double 
                 long long *nnz)
 {
     MPS_API_BODY(s, s->eng->get_ppe(eq_idx, row_ptr, col_idx, val, b, n_eq, nnz));
+}
+
+int mps_get_ic0(mps_session *s, int *row_ptr, int *col, double *A, double *F, double *b, int *n_eq,
+                long long *nnz)
+{
+    MPS_API_BODY(s, s->eng->get_ic0(row_ptr, col, A, F, b, n_eq, nnz));
+}
+
+int mps_get_cell_blocks(mps_session *s, int *cells, int *inv_off, double *inv, int *colour_rows, int *ncells,
+                        long long *ninv)
+{
+    MPS_API_BODY(s, s->eng->get_cell_blocks(cells, inv_off, inv, colour_rows, ncells, ninv));
+}
+
+int mps_apply_preconditioner(mps_session *s, const double *r, double *z)
+{
+    MPS_API_BODY(s, s->eng->apply_preconditioner(r, z));
 }
 
 int mps_get_metrics(mps_session *s, mps_metrics_t *m)

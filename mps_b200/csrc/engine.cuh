@@ -69,6 +69,11 @@ public:
     virtual void get_ppe(int *eq_idx, int *row_ptr, int *col, double *val, double *b, int *n_eq,
                          long long *nnz) = 0;
     virtual void run_stage(int stage, const int *nb, const int *cnt, int max_nb, double arg) = 0;
+    // the last step's PPE and IC(0) preconditioner in the solver's numbering
+    virtual void get_ic0(int *row_ptr, int *col, double *A, double *F, double *b, int *n_eq, long long *nnz) = 0;
+    virtual void get_cell_blocks(int *cells, int *inv_off, double *inv, int *colour_rows, int *ncells,
+                                 long long *ninv) = 0;
+    virtual void apply_preconditioner(const double *r, double *z) = 0;
     virtual cudaStream_t stream() const = 0;
     // differentiation form: checkpoints and the adjoint of one step
     virtual size_t state_bytes() const = 0;

@@ -910,10 +910,10 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
 // The cell's block inverse is staged in shared memory by one bulk copy per
 // warp, issued with the other loads before pdl_wait().
 
-constexpr int JW = 4;                 // warps (cells in flight) per CTA
+constexpr int JW = 4;                 // warps per cell (a CTA per cell)
 constexpr int JSTAGE_M = 40;          // cells of up to this many unknowns stage their block inverse
 constexpr int JSTAGE = ((JSTAGE_M * (JSTAGE_M + 1) / 2) + 3) & ~3;
-constexpr int JU = 8;                 // cross entries per lane and row loaded in one batch
+constexpr int JU = 4;                 // diagonals per warp loaded in one batch
 constexpr int JMAXL = 512;            // cross entries of one row, at most (the list's max_neighbors bound)
 constexpr int MBAR_DRAIN_POLLS = 1 << 26;
 
@@ -1017,105 +1017,123 @@ __global__ void __launch_bounds__(32 * JW)
 k_sweep_cell(int kbeg, int kend, const int2 *__restrict__ desc, const int *__restrict__ inv_off,
              const TM *__restrict__ inv, const int *__restrict__ pk_off, const int *__restrict__ pk_len,
              const TM *__restrict__ pk_val, const unsigned char *__restrict__ pk_k, const TM *__restrict__ dinv,
-             const int *__restrict__ xp, const int *__restrict__ jdc, const int *__restrict__ jdp,
-             const unsigned char *__restrict__ jperm, const int *__restrict__ xc, const TM *__restrict__ xf,
-             const double *rhs, double *x, const CGScalars *sc, int first_polls, unsigned *err)
+             const int *__restrict__ jdc, const int *__restrict__ jdp, const unsigned char *__restrict__ jperm,
+             const int *__restrict__ xc, const TM *__restrict__ xf, const double *rhs, double *x,
+             const CGScalars *sc, int first_polls, int trigger_from, unsigned *err)
 {
     using T = double;   // vectors and sums; TM is the storage type of the factor
-    __shared__ __align__(128) TM stage[JW][JSTAGE];
-    __shared__ T spart[JW][SWEEP_MAXM];
-    __shared__ __align__(8) unsigned long long bars[JW];
-    pdl_trigger();
+    __shared__ __align__(128) TM stage[JSTAGE];
+    __shared__ T sacc[JW][SWEEP_MAXM];
+    __shared__ T spart[SWEEP_MAXM];
+    __shared__ int sjd[JMAXL + 1];
+    __shared__ __align__(8) unsigned long long bar;
+    // CTAs of the grid's last wave let the next launch start at once; the
+    // others count as triggered when they exit
+    if ((int)blockIdx.x >= trigger_from) pdl_trigger();
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int kk = kbeg + blockIdx.x * JW + w;
-    if (kk >= kend) {   // warp-uniform; no block barrier in this kernel
-        pdl_wait();
-        return;
-    }
+    int kk = kbeg + blockIdx.x;   // grid = cells of the colour
     int2 dd = __ldg(&desc[kk]);
     int r0 = dd.x, m = dd.y;
     int io = __ldg(&inv_off[kk]);
     int nb = __ldg(&inv_off[kk + 1]) - io;
     bool staged = m <= JSTAGE_M && nb > 0;
-    unsigned bar = smem_u32(&bars[w]);
-    if (staged && lane == 0) {
-        mbar_init(bar, 1);
-        mbar_arrive_expect_tx(bar, (unsigned)nb * (unsigned)sizeof(TM));
-        bulk_g2s(smem_u32(stage[w]), inv + io, (unsigned)nb * (unsigned)sizeof(TM), bar);
+    unsigned b = smem_u32(&bar);
+    if (staged && threadIdx.x == 0) {
+        mbar_init(b, 1);
+        mbar_arrive_expect_tx(b, (unsigned)nb * (unsigned)sizeof(TM));
+        bulk_g2s(smem_u32(stage), inv + io, (unsigned)nb * (unsigned)sizeof(TM), b);
     }
     int jb = __ldg(&jdc[kk]);
-    // the first batch of the lane's first row (rank = lane): factor values
-    // and columns are written once per step, before the CG loop
-    int i0 = 0, len0 = 0;
-    TM f[JU];
-    int c[JU];
-    if (lane < m) {
-        i0 = __ldg(&jperm[r0 + lane]);
-        len0 = __ldg(&xp[r0 + i0 + 1]) - __ldg(&xp[r0 + i0]);
-    }
+    int nk = __ldg(&jdc[kk + 1]) - jb - 1;   // diagonals
+    for (int k = threadIdx.x; k <= nk; k += 32 * JW) sjd[k] = __ldg(&jdp[jb + k]);
+    __syncthreads();
+    // warp w takes diagonals w, w + JW, ...; lane q the row of rank q (and
+    // q + 32); the first batch is loaded before the dependency wait (factor
+    // values and columns are written once per step, before the CG loop)
+    TM f[JU][2];
+    int c[JU][2];
+    auto load = [&](int k0) {
 #pragma unroll
-    for (int u = 0; u < JU; u++) {
-        bool ok = u < len0;
-        int q = ok ? __ldg(&jdp[jb + u]) + lane : 0;
-        f[u] = ok ? __ldg(&xf[q]) : TM(0);
-        c[u] = ok ? __ldg(&xc[q]) : -1;
-    }
+        for (int u = 0; u < JU; u++) {
+            int k = k0 + u * JW;
+            int a = k < nk ? sjd[k] : 0, cnt = k < nk ? sjd[k + 1] - a : 0;
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                int q = lane + 32 * h;
+                bool ok = q < cnt;
+                f[u][h] = ok ? __ldg(&xf[a + q]) : TM(0);
+                c[u][h] = ok ? __ldg(&xc[a + q]) : -1;
+            }
+        }
+    };
+    load(w);
     pdl_wait();
     if (sc->done) {
-        if (staged) stage_wait(bar, MBAR_DRAIN_POLLS, err);
+        if (staged && threadIdx.x == 0) stage_wait(b, MBAR_DRAIN_POLLS, err);
         return;
     }
-    const bool big = m > SWEEP_MAXM;   // substitution in place in x (only in a blow-up)
-    for (int q0 = lane; q0 < m; q0 += 32) {
-        int i = q0 == lane ? i0 : __ldg(&jperm[r0 + q0]);
-        int len = q0 == lane ? len0 : __ldg(&xp[r0 + i + 1]) - __ldg(&xp[r0 + i]);
-        T s = T(0);
-        for (int k0 = 0; k0 < len; k0 += JU) {
-            if (k0 > 0 || q0 != lane) {
+    T s0 = T(0), s1 = T(0);
+    for (int k0 = w; k0 < nk; k0 += JU * JW) {
+        if (k0 != w) load(k0);
 #pragma unroll
-                for (int u = 0; u < JU; u++) {
-                    bool ok = k0 + u < len;
-                    int q = ok ? __ldg(&jdp[jb + k0 + u]) + q0 : 0;
-                    f[u] = ok ? __ldg(&xf[q]) : TM(0);
-                    c[u] = ok ? __ldg(&xc[q]) : -1;
-                }
+        for (int u = 0; u < JU; u++) {
+            if (c[u][0] >= 0) s0 += T(f[u][0]) * x[c[u][0]];
+            if (c[u][1] >= 0) s1 += T(f[u][1]) * x[c[u][1]];
+        }
+    }
+    if (m > SWEEP_MAXM) {
+        // only in a blow-up: rank by rank cross sums (thread per rank, in
+        // diagonal order) into x, then substitution in place
+        for (int q = threadIdx.x; q < m; q += 32 * JW) {
+            T v = T(0);
+            for (int k = 0; k < nk && q < sjd[k + 1] - sjd[k]; k++) {
+                int e = sjd[k] + q;
+                v += T(__ldg(&xf[e])) * x[__ldg(&xc[e])];
             }
-#pragma unroll
-            for (int u = 0; u < JU; u++)
-                if (c[u] >= 0) s += T(f[u]) * x[c[u]];
+            int i = __ldg(&jperm[r0 + q]);
+            x[r0 + i] = rhs[r0 + i] - v;
         }
-        T pv = rhs[r0 + i] - s;
-        if (big) x[r0 + i] = pv;
-        else spart[w][i] = pv;
-    }
-    if (big) {
         __threadfence_block();
-        __syncwarp();
-        for (int t = 0; t < m; t++) {
-            int r = FWD ? r0 + t : r0 + m - 1 - t;
-            int po = pk_off[r], l = pk_len[r];
-            T ps = T(0);
-            for (int e = lane; e < l; e += 32) ps += T(pk_val[po + e]) * x[r0 + pk_k[po + e]];
+        __syncthreads();
+        if (w == 0) {
+            for (int t = 0; t < m; t++) {
+                int r = FWD ? r0 + t : r0 + m - 1 - t;
+                int po = pk_off[r], l = pk_len[r];
+                T ps = T(0);
+                for (int e = lane; e < l; e += 32) ps += T(pk_val[po + e]) * x[r0 + pk_k[po + e]];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, o);
-            if (lane == 0) x[r] = (x[r] - ps) * T(dinv[r]);
-            __threadfence_block();
-            __syncwarp();
+                for (int o = 16; o > 0; o >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, o);
+                if (lane == 0) x[r] = (x[r] - ps) * T(dinv[r]);
+                __threadfence_block();
+                __syncwarp();
+            }
         }
         return;
     }
-    __syncwarp();
+    sacc[w][lane] = s0;
+    sacc[w][lane + 32] = s1;
+    __syncthreads();
+    if (threadIdx.x < m) {
+        int q = threadIdx.x;
+        T t = T(0);
+#pragma unroll
+        for (int ww = 0; ww < JW; ww++) t += sacc[ww][q];
+        int i = __ldg(&jperm[r0 + q]);
+        spart[i] = rhs[r0 + i] - t;
+    }
+    __syncthreads();
     const TM *blk = inv + io;
     if (staged) {
-        if (!stage_wait(bar, first_polls, err)) return;
-        blk = stage[w];
+        if (!stage_wait(b, first_polls, err)) return;
+        blk = stage;
     }
-    for (int i = lane; i < m; i += 32) {
+    // in-cell product, a thread per row
+    for (int i = threadIdx.x; i < m; i += 32 * JW) {
         T y = T(0);
         if (FWD) {
-            for (int j = 0; j <= i; j++) y += T(blk[tri_colofs(j, m) + i - j]) * spart[w][j];
+            for (int j = 0; j <= i; j++) y += T(blk[tri_colofs(j, m) + i - j]) * spart[j];
         } else {
-            for (int j = i; j < m; j++) y += T(blk[j * (j + 1) / 2 + i]) * spart[w][j];
+            for (int j = i; j < m; j++) y += T(blk[j * (j + 1) / 2 + i]) * spart[j];
         }
         x[r0 + i] = y;
     }

@@ -144,6 +144,40 @@ class Session:
                                          b.ctypes.data, C.byref(n_eq), C.byref(nnz)))
         return eq, rp, ci[: nnz.value], va[: nnz.value], b[: n_eq.value]
 
+    def ic0(self):
+        """The last step's PPE and IC(0) factor in the solver's numbering:
+        dict of row_ptr, col, A, F, b (numpy)."""
+        n_eq, nnz = C.c_int(), C.c_longlong()
+        self._check(self.lib.mps_get_ic0(self.h, None, None, None, None, None, C.byref(n_eq), C.byref(nnz)))
+        ne, nz = n_eq.value, nnz.value
+        rp = np.zeros(ne + 1, dtype=np.int32)
+        ci = np.zeros(nz, dtype=np.int32)
+        A = np.zeros(nz)
+        F = np.zeros(nz)
+        b = np.zeros(ne)
+        self._check(self.lib.mps_get_ic0(self.h, rp.ctypes.data, ci.ctypes.data, A.ctypes.data, F.ctypes.data,
+                                         b.ctypes.data, C.byref(n_eq), C.byref(nnz)))
+        return {"row_ptr": rp, "col": ci, "A": A, "F": F, "b": b}
+
+    def cell_blocks(self):
+        """(cells (ncells, 2) [first row, unknowns], inv_off, inv, colour_rows)."""
+        nc, ninv = C.c_int(), C.c_longlong()
+        cr = np.zeros(9, dtype=np.int32)
+        self._check(self.lib.mps_get_cell_blocks(self.h, None, None, None, cr.ctypes.data, C.byref(nc),
+                                                 C.byref(ninv)))
+        cells = np.zeros((nc.value, 2), dtype=np.int32)
+        off = np.zeros(nc.value + 1, dtype=np.int32)
+        inv = np.zeros(max(ninv.value, 1))
+        self._check(self.lib.mps_get_cell_blocks(self.h, cells.ctypes.data, off.ctypes.data, inv.ctypes.data,
+                                                 cr.ctypes.data, C.byref(nc), C.byref(ninv)))
+        return cells, off, inv, cr[: (1 << self.dim) + 1]
+
+    def apply_preconditioner(self, r):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.zeros_like(r)
+        self._check(self.lib.mps_apply_preconditioner(self.h, r.ctypes.data, z.ctypes.data))
+        return z
+
     def metrics(self) -> dict:
         m = _lib.MpsMetrics()
         self._check(self.lib.mps_get_metrics(self.h, C.byref(m)))

@@ -773,6 +773,105 @@ static int ic0_factor(const Csr *A, const double *diag, Lfac *L)
     return 0;
 }
 
+/* IC(0) of a CSR matrix (sorted columns, diagonal included) in its own row
+ * order, the algorithm of pressure_solver.c:156-232 (ic0_factor above) on
+ * whatever unknown numbering the caller gives: here the GPU solver's block
+ * colour order.  F receives the factor in A's pattern as that solver stores
+ * it: L_ij below the diagonal, 1/L_ii on it, L_ji above it.  0, -1 on OOM. */
+int oracle_ic0_csr(int n, const int *rp, const int *ci, const double *v, double *F)
+{
+    Csr A = {n, rp, ci, v};
+    double *diag = calloc((size_t)(n + 1), sizeof(double));
+    if (!diag) return -1;
+    for (int i = 0; i < n; i++) {
+        for (int p = rp[i]; p < rp[i + 1]; p++) if (ci[p] == i) diag[i] = v[p];
+    }
+    Lfac L;
+    if (ic0_factor(&A, diag, &L) != 0) { free(diag); return -1; }
+    for (int i = 0; i < n; i++) {
+        int q = L.rp[i];
+        for (int p = rp[i]; p < rp[i + 1]; p++) {
+            int j = ci[p];
+            if (j < i) F[p] = L.v[q++];
+            else if (j == i) F[p] = L.dinv[i];
+            else {
+                /* L_ji: row j's lower entry in column i */
+                int lo = L.rp[j], hi = L.rp[j + 1];
+                double f = 0.0;
+                while (lo < hi) {
+                    int mid = (lo + hi) / 2;
+                    if (L.ci[mid] == i) { f = L.v[mid]; break; }
+                    if (L.ci[mid] < i) lo = mid + 1; else hi = mid;
+                }
+                F[p] = f;
+            }
+        }
+    }
+    lfac_free(&L);
+    free(diag);
+    return 0;
+}
+
+/* The inverse of each cell's diagonal block of L, the factor F in the
+ * solver's convention: cells[2k] = first row r0, cells[2k+1] = unknowns m;
+ * column-major lower triangle at inv + inv_off[k]: X_ij (i >= j) at
+ * j*m - j*(j-1)/2 + (i - j), by forward substitution column by column,
+ * X_ic = (delta_ic - sum_{c <= k < i} L_ik X_kc) / L_ii.  Cells above
+ * max_m unknowns are skipped. */
+void oracle_cell_inverses(int ncells, const int *cells, const int *inv_off, const int *rp, const int *ci,
+                          const double *F, int max_m, double *inv)
+{
+    for (int k = 0; k < ncells; k++) {
+        int r0 = cells[2 * k], m = cells[2 * k + 1];
+        if (m > max_m) continue;
+        double *X = inv + inv_off[k];
+        double *Ld = malloc(sizeof(double) * (size_t)m * (size_t)m);
+        if (!Ld) return;
+        for (int i = 0; i < m * m; i++) Ld[i] = 0.0;
+        for (int i = 0; i < m; i++)
+            for (int p = rp[r0 + i]; p < rp[r0 + i + 1]; p++) {
+                int j = ci[p] - r0;
+                if (j >= 0 && j < i) Ld[i * m + j] = F[p];
+                if (j == i) Ld[i * m + i] = F[p];   /* 1 / L_ii */
+            }
+        for (int c = 0; c < m; c++) {
+            int off = c * m - (c * (c - 1)) / 2;
+            for (int i = c; i < m; i++) {
+                double s = (i == c) ? 1.0 : 0.0;
+                for (int kk = c; kk < i; kk++) s -= Ld[i * m + kk] * X[off + kk - c];
+                X[off + i - c] = s * Ld[i * m + i];
+            }
+        }
+        free(Ld);
+    }
+}
+
+/* z = (L L^T)^-1 r with the factor F in the solver's convention: forward
+ * L y = r over the lower entries, backward L^T z = y over the upper copy
+ * (the sweeps of pressure_solver.c:235-255). */
+void oracle_ic0_apply_csr(int n, const int *rp, const int *ci, const double *F, const double *r, double *z)
+{
+    double *y = malloc(sizeof(double) * (size_t)(n + 1));
+    if (!y) return;
+    for (int i = 0; i < n; i++) {
+        double s = r[i], d = 0.0;
+        for (int p = rp[i]; p < rp[i + 1]; p++) {
+            if (ci[p] < i) s -= F[p] * y[ci[p]];
+            else if (ci[p] == i) d = F[p];
+        }
+        y[i] = s * d;
+    }
+    for (int i = n - 1; i >= 0; i--) {
+        double s = y[i], d = 0.0;
+        for (int p = rp[i]; p < rp[i + 1]; p++) {
+            if (ci[p] > i) s -= F[p] * z[ci[p]];
+            else if (ci[p] == i) d = F[p];
+        }
+        z[i] = s * d;
+    }
+    free(y);
+}
+
 /* Forward L y = r and backward L^T z = y (scatter form), 3P :235-255. */
 static void ic0_apply(const Lfac *L, const double *r, double *tmp, double *z)
 {

@@ -66,6 +66,15 @@ int  oracle_step_driven(ParticleSystem *ps, NeighborList *nl, CellList *cl, cons
                         const double *rest, double amp, double freq, int axis, int step);
 void oracle_wall_drive_terms(double amp, double freq, double t, double *dx, double *vel);
 
+/* IC(0) on any unknown numbering (pressure_solver.c:156-232 applied to the
+ * caller's CSR, e.g. the GPU solver's block colour order), the in-cell block
+ * inverses and the preconditioner apply, in the GPU solver's factor
+ * convention (F: L below the diagonal, 1/L_ii on it, L^T above). */
+int  oracle_ic0_csr(int n, const int *rp, const int *ci, const double *v, double *F);
+void oracle_cell_inverses(int ncells, const int *cells, const int *inv_off, const int *rp, const int *ci,
+                          const double *F, int max_m, double *inv);
+void oracle_ic0_apply_csr(int n, const int *rp, const int *ci, const double *F, const double *r, double *z);
+
 /* Iteration count and final recursive residual of the last PPE solve. */
 int    oracle_last_iterations(void);
 double oracle_last_residual(void);

@@ -69,6 +69,9 @@ class Oracle:
             "oracle_remove_out_of_bounds": (None, [PS, CF]),
             "oracle_step": (C.c_int, [PS, NL, CL, CF]),
             "oracle_step_driven": (C.c_int, [PS, NL, CL, CF, P, C.c_double, C.c_double, C.c_int, C.c_int]),
+            "oracle_ic0_csr": (C.c_int, [C.c_int, P, P, P, P]),
+            "oracle_cell_inverses": (None, [C.c_int, P, P, P, P, P, C.c_int, P]),
+            "oracle_ic0_apply_csr": (None, [C.c_int, P, P, P, P, P]),
             "oracle_last_iterations": (C.c_int, []),
             "oracle_last_residual": (C.c_double, []),
         }
@@ -78,6 +81,38 @@ class Oracle:
             f.argtypes = args
 
     # --- convenience wrappers -------------------------------------------------
+    def ic0_csr(self, rp, ci, v):
+        """IC(0) of a CSR matrix in its own numbering; the factor in A's
+        pattern (L below, 1/L_ii on, L^T above the diagonal)."""
+        rp = np.ascontiguousarray(rp, dtype=np.int32)
+        ci = np.ascontiguousarray(ci, dtype=np.int32)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        F = np.zeros_like(v)
+        if self.lib.oracle_ic0_csr(len(rp) - 1, rp.ctypes.data, ci.ctypes.data, v.ctypes.data, F.ctypes.data):
+            raise MemoryError("oracle_ic0_csr")
+        return F
+
+    def cell_inverses(self, cells, inv_off, rp, ci, F, max_m=64):
+        cells = np.ascontiguousarray(cells, dtype=np.int32)
+        inv_off = np.ascontiguousarray(inv_off, dtype=np.int32)
+        rp = np.ascontiguousarray(rp, dtype=np.int32)
+        ci = np.ascontiguousarray(ci, dtype=np.int32)
+        F = np.ascontiguousarray(F, dtype=np.float64)
+        inv = np.zeros(max(int(inv_off[-1]), 1))
+        self.lib.oracle_cell_inverses(len(cells), cells.ctypes.data, inv_off.ctypes.data, rp.ctypes.data,
+                                      ci.ctypes.data, F.ctypes.data, int(max_m), inv.ctypes.data)
+        return inv
+
+    def ic0_apply_csr(self, rp, ci, F, r):
+        rp = np.ascontiguousarray(rp, dtype=np.int32)
+        ci = np.ascontiguousarray(ci, dtype=np.int32)
+        F = np.ascontiguousarray(F, dtype=np.float64)
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        z = np.zeros_like(r)
+        self.lib.oracle_ic0_apply_csr(len(rp) - 1, rp.ctypes.data, ci.ctypes.data, F.ctypes.data, r.ctypes.data,
+                                      z.ctypes.data)
+        return z
+
     def cell_list(self, num: int, re: float, cfg):
         cl = T.cell_list_type(self.dim)()
         dmin = (C.c_double * self.dim)(*cfg.domain_min)
