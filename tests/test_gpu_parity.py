@@ -346,9 +346,11 @@ def test_mixed_precision_against_fp64(steps):
     """The mixed form (PPE matrix and IC(0) factor stored in FP32, FP64
     vectors, reliable updates against the FP64 matrix) stays within the
     1e-4 pressure relative-L2 target of the FP64 path, from the same state,
-    and ends its solve at the residual level the FP64 path reaches: the true
-    residual ||b - A x|| within 4x the FP64 rounding floor (or below the
-    1e-9 tolerance) and within 1.5x of the FP64 path's own."""
+    and ends its solves at the residual level the FP64 path reaches: every
+    step's true residual ||b - A x|| within 4x the FP64 rounding floor (or
+    below the 1e-9 tolerance), and the mean over the steps within 1.5x of
+    the FP64 path's mean (the FP64 solve's end residual, set by its
+    recursive test, varies by a few rounding floors from step to step)."""
     _cuda()
     from mps_b200 import _lib
     from mps_b200.session import start
@@ -358,19 +360,23 @@ def test_mixed_precision_against_fp64(steps):
     h32 = h64.copy()
     a = start(cfg, 3, h64)
     b = start(cfg, 3, h32, precision=_lib.PREC_MIXED)
-    a.step(steps)
-    b.step(steps)
+    tra, trb = [], []
+    for _ in range(steps):
+        a.step(1)
+        b.step(1)
+        ma, mb = a.metrics(), b.metrics()
+        assert mb["ppe_outer"] >= 1 and mb["converged"] == 1
+        assert mb["ppe_true_residual"] <= max(cfg.cg_tolerance, 4.0 * mb["ppe_rounding_floor"])
+        assert ma["ppe_true_residual"] > 0.0 and ma["ppe_rounding_floor"] > 0.0
+        tra.append(ma["ppe_true_residual"])
+        trb.append(mb["ppe_true_residual"])
     ga, gb = a.download(), b.download()
-    ma, mb = a.metrics(), b.metrics()
     a.close()
     b.close()
     assert np.array_equal(ga["type"], gb["type"])
     assert _rel(gb["pressure"], ga["pressure"]) < 1e-4
     assert _rel(gb["pos"], ga["pos"]) < 1e-6
-    assert mb["ppe_outer"] >= 1 and mb["converged"] == 1
-    assert mb["ppe_true_residual"] <= max(cfg.cg_tolerance, 4.0 * mb["ppe_rounding_floor"])
-    assert mb["ppe_true_residual"] <= max(cfg.cg_tolerance, 1.5 * ma["ppe_true_residual"])
-    assert ma["ppe_true_residual"] > 0.0 and ma["ppe_rounding_floor"] > 0.0
+    assert np.mean(trb) <= max(cfg.cg_tolerance, 1.5 * np.mean(tra))
 
 
 def test_set_precision_switches_the_form():
