@@ -136,6 +136,12 @@ typedef struct {
     long long sweep_cross_lo;
     long long sweep_cross_up;
     long long sweep_inverse_entries;
+    /* Device time of the persistent ICCG kernel (one cooperative launch per
+     * batch of CG iterations) summed over the session while profiling is
+     * on, its launches and the iterations they ran. */
+    double prof_pcg_ms;
+    long long prof_pcg_launches;
+    long long prof_pcg_iterations;
 } mps_metrics_t;
 
 typedef struct mps_session mps_session;

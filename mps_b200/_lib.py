@@ -118,6 +118,9 @@ class MpsMetrics(C.Structure):
         ("sweep_cross_lo", C.c_longlong),
         ("sweep_cross_up", C.c_longlong),
         ("sweep_inverse_entries", C.c_longlong),
+        ("prof_pcg_ms", C.c_double),
+        ("prof_pcg_launches", C.c_longlong),
+        ("prof_pcg_iterations", C.c_longlong),
     ]
 
 

@@ -82,6 +82,7 @@ enum : unsigned {
     ERR_CELL_OVERFULL     = 16u,  // more than 255 unknowns in one cell
     ERR_COPY_TIMEOUT      = 32u,  // a bulk copy into shared memory did not complete in time
     ERR_WINDOW_OVERFLOW   = 64u,  // a window of block inverses exceeded its shared-memory stage
+    ERR_GRID_TIMEOUT      = 128u, // a grid barrier of the persistent PCG kernel did not complete in time
 };
 
 // Constants of one session, evaluated on the host with the reference's

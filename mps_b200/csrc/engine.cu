@@ -29,6 +29,7 @@
 #include "engine.cuh"
 #include "k_ops.cuh"
 #include "k_ppe.cuh"
+#include "k_pcg.cuh"
 #include "k_sort.cuh"
 #include "k_adj.cuh"
 
@@ -241,9 +242,17 @@ private:
     // cell (jlen_, its scan jdc_*), diagonal slots (jdp_*), row of each rank
     DevArray<int> jlen_, jdc_lo_, jdc_up_, jdp_lo_, jdp_up_;
     DevArray<unsigned char> jperm_lo_, jperm_up_;
-    // sweep kernel (MPS_SWEEP): 0 the windowed k_sweep_colour (default), 1
-    // the CTA-per-cell k_sweep_cell over jagged-diagonal cross blocks
+    // ICCG loop (MPS_SWEEP): 2 the persistent k_pcg (one cooperative launch
+    // per batch of iterations), 0 the launch-per-colour k_sweep_colour with
+    // separate SpMV and vector kernels, 1 the same with the CTA-per-cell
+    // k_sweep_cell over jagged-diagonal cross blocks
     int sweep_mode_ = 0;
+    DevArray<unsigned> pcg_bar_;   // grid-barrier counter of k_pcg
+    int pcg_batch_ = 16;           // k_pcg iterations per launch (MPS_PCG_BATCH)
+    int pcg_grid_[3] = {0, 0, 0};  // k_pcg grid per variant (FP64; FP32 difference form; FP32)
+    // polls of a k_pcg grid-barrier wait (MPS_TEST_BAR_POLLS lowers it, down
+    // to 0, to exercise the timeout path)
+    int bar_polls_ = PCG_BAR_POLLS;
     // polls of the first wait for a staged block inverse (MPS_TEST_MBAR_POLLS
     // lowers it, down to 0, to exercise the timeout path)
     int first_polls_ = MBAR_POLLS;
@@ -256,7 +265,7 @@ private:
 
     // ---- PPE
     DevArray<int> ucount_, ucol_, rs_, cell_row0_, row_of_, part_of_row_, rcount_, row_ptr_, diagpos_, col_;
-    DevArray<double> A_, F_, b_, x_, r_, z_, p_, Ap_, y_, part_, partials_;
+    DevArray<double> A_, F_, b_, x_, r_, z_, p_, Ap_, y_, part_, partials_, p2_;
     DevArray<float> A32_, xf32_lo_, xf32_up_, pkv32_lo_, pkv32_up_, inv32_cm_, inv32_rm_, dinv32_;
     DevArray<double> zprev_, dsum_;
     DevArray<CGScalars> sc_;
@@ -348,6 +357,11 @@ private:
                    const double *zprev = nullptr);
     template <class TM>
     void run_sweep(const PcgBufs<TM> &v, bool fwdir);
+    // one cooperative launch of k_pcg: `batch` CG iterations, or (apply) the
+    // two sweeps z = M^-1 r only
+    template <class TM>
+    void launch_pcg(const PcgBufs<TM> &v, bool apply, int batch);
+    int pcg_grid(const void *kernel);
     void mixed_solve(int n_eq, long long nnz, bool icc);
     void build_windows(bool fp32);
     static constexpr int kMaxUpdates = 200;      // reliable updates of the mixed form, at most
@@ -390,7 +404,18 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
         if (v > 0.0 && v < 1.0) rel_delta_ = v;
     }
     if (const char *e = std::getenv("MPS_MIXED_SPMV")) mixed_spmv_ = std::atoi(e);
-    if (const char *e = std::getenv("MPS_SWEEP")) sweep_mode_ = std::atoi(e) == 1 ? 1 : 0;
+    if (const char *e = std::getenv("MPS_SWEEP")) {
+        int v = std::atoi(e);
+        sweep_mode_ = (v == 0 || v == 1) ? v : 2;
+    }
+    if (const char *e = std::getenv("MPS_PCG_BATCH")) {
+        int v = std::atoi(e);
+        if (v >= 1 && v <= 1024) pcg_batch_ = v;
+    }
+    if (const char *e = std::getenv("MPS_TEST_BAR_POLLS")) {
+        int v = std::atoi(e);
+        if (v >= 0 && v < PCG_BAR_POLLS) bar_polls_ = v;
+    }
     if (const char *e = std::getenv("MPS_CELL_EARLY")) cell_early_ = std::atoi(e) != 0;
     {
         int dev = 0;
@@ -422,6 +447,7 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
     sc_.reserve(1);
     ticket_.reserve(4);
     err_.reserve(1);
+    pcg_bar_.reserve(1);
     partials_.reserve(6 * RED_BLOCKS + 8);
     MPS_CUDA(cudaMemsetAsync(ticket_.p, 0, 4 * sizeof(unsigned), st_));
     MPS_CUDA(cudaMemsetAsync(err_.p, 0, sizeof(unsigned), st_));
@@ -506,7 +532,7 @@ void Engine<D>::alloc_state()
     outpos_.reserve(cap_);
     for (auto *v : {&pk_len_lo_, &pk_len_up_, &pk_off_lo_, &pk_off_up_}) v->reserve((size_t)cap_ + 1);
     dinv_.reserve(cap_);
-    for (auto *v : {&b_, &x_, &r_, &z_, &p_, &Ap_, &y_, &part_}) v->reserve(cap_);
+    for (auto *v : {&b_, &x_, &r_, &z_, &p_, &Ap_, &y_, &part_, &p2_}) v->reserve(cap_);
 }
 
 // cell_list_create (neighbor_search.c:92-122) with cell size = list radius.
@@ -658,6 +684,7 @@ void Engine<D>::check_err()
         if (e & ERR_COLORING) throw CudaError("PPE row count mismatch", MPS_ERR_INVALID);
         if (e & ERR_CELL_OVERFULL) throw CudaError("more than 255 PPE unknowns in one cell", MPS_ERR_UNSUPPORTED);
         if (e & ERR_COPY_TIMEOUT) throw CudaError("a bulk copy into shared memory timed out", MPS_ERR_CUDA);
+        if (e & ERR_GRID_TIMEOUT) throw CudaError("a grid barrier of the persistent PCG kernel timed out", MPS_ERR_CUDA);
         if (e & ERR_WINDOW_OVERFLOW) throw CudaError("in-cell inverse window exceeds its stage", MPS_ERR_INVALID);
         throw CudaError("device error", MPS_ERR_INVALID);
     }
@@ -1132,8 +1159,8 @@ void Engine<D>::ppe(bool clamp)
         if (nact)
             launch(k_cell_desc, nblk(nact, TPB), TPB, 0, st_, nact, (const int *)acells_.p,
                    (const int *)cell_row0_.p, (const int *)ucount_.p, adesc_.p);
-        if (sweep_mode_ == 1) {
-            // the cross runs of each cell in jagged-diagonal order (k_sweep_cell)
+        if (sweep_mode_ != 0) {
+            // the cross runs of each cell in jagged-diagonal order (k_sweep_cell, k_pcg)
             for (auto *v : {&jlen_, &jdc_lo_, &jdc_up_}) v->reserve((size_t)nact + 1);
             for (auto *v : {&jperm_lo_, &jperm_up_}) v->reserve((size_t)n_eq + 1);
             for (int lo = 1; lo >= 0; lo--) {
@@ -1333,13 +1360,49 @@ void Engine<D>::pcg_solve(const PcgBufs<TM> &v, double tol, int maxit, bool icc,
             lk(4, k_cg_spmv<8, TM>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
                ticket_.p, sc_.p, (const double *)nullptr);
     };
-    if (icc) { sweep(true); sweep(false); }
+    const bool persist = icc && sweep_mode_ == 2;
+    if (icc) {
+        if (persist) launch_pcg<TM>(v, true, 0);
+        else {
+            sweep(true);
+            sweep(false);
+        }
+    }
     if (!zprev)
         launch(k_cg_init2<T>, RB, CG_BLOCK, 0, st_, n_eq, (const T *)v.r, (const T *)z, v.p, partials_.p, ticket_.p,
                sc_.p);
     else
         launch(k_reliable_fix<T>, RB, CG_BLOCK, 0, st_, n_eq, (const T *)v.r, (const T *)z, zprev, v.p, tol,
                partials_.p, ticket_.p, sc_.p);
+    if (persist) {
+        // one cooperative launch per batch; the kernel stops by itself at
+        // convergence, so the host only reads the scalars between batches
+        for (;;) {
+            bool prof = profiling;
+            if (prof) MPS_CUDA(cudaEventRecord(pev_[0], st_));
+            launch_pcg<TM>(v, false, pcg_batch_);
+            if (prof) MPS_CUDA(cudaEventRecord(pev_[1], st_));
+            MPS_CUDA(cudaGetLastError());
+            MPS_CUDA(cudaMemcpyAsync(sc_host_, sc_.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, st_));
+            MPS_CUDA(cudaMemcpyAsync(int_host_ + 60, err_.p, sizeof(unsigned), cudaMemcpyDeviceToHost, st_));
+            MPS_CUDA(cudaStreamSynchronize(st_));
+            if (int_host_[60]) check_err();
+            int worked = sc_host_->iter - iter_before;
+            if (prof) {
+                float ms = 0;
+                cudaEventElapsedTime(&ms, pev_[0], pev_[1]);
+                met.prof_pcg_ms += ms;
+                met.prof_pcg_launches += 1;
+                met.prof_pcg_iterations += worked;
+                met.prof_iterations += worked;
+                met.prof_nnz_sum += (long long)worked * nnz;
+                met.prof_rows_sum += (long long)worked * n_eq;
+            }
+            iter_before = sc_host_->iter;
+            if (sc_host_->done) break;
+        }
+        return;
+    }
     for (;;) {
         bool prof = profiling;
         for (int it = 0; it < CG_BATCH; it++) {
@@ -1386,6 +1449,99 @@ void Engine<D>::pcg_solve(const PcgBufs<TM> &v, double tol, int maxit, bool icc,
         iter_before = sc_host_->iter;
         if (sc_host_->done) break;
     }
+}
+
+// Grid of k_pcg: every CTA must be resident at once (the grid barriers wait
+// for all of them), so the grid is the occupancy, at most 2 CTAs per SM,
+// times the SM count; a cooperative launch refuses anything larger.
+template <int D>
+int Engine<D>::pcg_grid(const void *kernel)
+{
+    int nb = 0;
+    MPS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, PCG_THREADS, 0));
+    nb = std::min(nb, 2);
+    if (nb < 1) throw CudaError("the persistent PCG kernel cannot be resident", MPS_ERR_CUDA);
+    return nb * num_sms_;
+}
+
+template <int D>
+template <class TM>
+void Engine<D>::launch_pcg(const PcgBufs<TM> &v, bool apply, int batch)
+{
+    PcgArgs<TM> a{};
+    int nc = 0;
+    for (int c = 0; c < (1 << D); c++)
+        if (act_off_[c + 1] > act_off_[c]) {
+            a.kb[nc] = act_off_[c];
+            a.ke[nc] = act_off_[c + 1];
+            nc++;
+        }
+    if (nc == 0) return;
+    if (v.A64) throw CudaError("the persistent PCG kernel reads the matrix in its storage type only", MPS_ERR_UNSUPPORTED);
+    a.n_eq = n_eq_;
+    a.ncol = nc;
+    a.row_ptr = row_ptr_.p;
+    a.colidx = col_.p;
+    a.A = v.A;
+    a.dsum = v.dsum;
+    a.desc = adesc_.p;
+    a.inv_off = inv_off_.p;
+    a.inv_cm = v.inv_cm;
+    a.inv_rm = v.inv_rm;
+    a.jdc_lo = jdc_lo_.p;
+    a.jdp_lo = jdp_lo_.p;
+    a.jdc_up = jdc_up_.p;
+    a.jdp_up = jdp_up_.p;
+    a.jperm_lo = jperm_lo_.p;
+    a.jperm_up = jperm_up_.p;
+    a.xc_lo = xc_lo_.p;
+    a.xc_up = xc_up_.p;
+    a.xf_lo = v.xf_lo;
+    a.xf_up = v.xf_up;
+    a.pk_off_lo = pk_off_lo_.p;
+    a.pk_len_lo = pk_len_lo_.p;
+    a.pk_off_up = pk_off_up_.p;
+    a.pk_len_up = pk_len_up_.p;
+    a.pkv_lo = v.pkv_lo;
+    a.pkv_up = v.pkv_up;
+    a.pkk_lo = pk_k_lo_.p;
+    a.pkk_up = pk_k_up_.p;
+    a.dinv = v.dinv;
+    a.x = v.x;
+    a.r = v.r;
+    a.y = v.y;
+    a.z = v.z;
+    a.Ap = v.Ap;
+    a.p = v.p;
+    a.p2 = p2_.p;
+    a.sc = sc_.p;
+    a.partials = partials_.p;
+    a.bar = pcg_bar_.p;
+    a.err = err_.p;
+    a.batch = batch;
+    a.apply = apply ? 1 : 0;
+    a.bar_polls = bar_polls_;
+    const void *k;
+    int variant;
+    if constexpr (sizeof(TM) == 8) {
+        k = (const void *)k_pcg<TM, false>;
+        variant = 0;
+    } else {
+        if (v.dsum) {
+            k = (const void *)k_pcg<TM, true>;
+            variant = 1;
+        } else {
+            k = (const void *)k_pcg<TM, false>;
+            variant = 2;
+        }
+    }
+    if (!pcg_grid_[variant]) pcg_grid_[variant] = pcg_grid(k);
+    int grid = pcg_grid_[variant];
+    if ((size_t)PCG_SLOTS * grid > partials_.n) throw CudaError("PCG partials too small", MPS_ERR_CUDA);
+    MPS_CUDA(cudaMemsetAsync(pcg_bar_.p, 0, sizeof(unsigned), st_));
+    void *args[] = {&a};
+    MPS_CUDA(cudaLaunchCooperativeKernel(k, grid, PCG_THREADS, args, 0, st_));
+    ++launch_counter();
 }
 
 // Window tables of the staged in-cell sweeps for the current factor: each
@@ -1461,7 +1617,7 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
     PcgBufs<float> v{A32_.p,      xf32_lo_.p, xf32_up_.p, pkv32_lo_.p, pkv32_up_.p, dinv32_.p, inv32_cm_.p,
                      inv32_rm_.p, x_.p,       r_.p,       z_.p,        p_.p,        Ap_.p,     y_.p,
                      part_.p,     b_.p};
-    if (mixed_spmv_ == 1) v.A64 = A_.p;   // tuning alternatives of the inner SpMV
+    if (mixed_spmv_ == 1 && sweep_mode_ != 2) v.A64 = A_.p;   // tuning alternatives of the inner SpMV
     if (mixed_spmv_ == 2) {
         dsum_.reserve((size_t)cap_);
         launch(k_row_sum, nblk(n_eq, TPB), TPB, 0, st_, n_eq, (const int *)row_ptr_.p, (const double *)A_.p,
@@ -1962,15 +2118,21 @@ void Engine<D>::apply_preconditioner(const double *r, double *z)
         PcgBufs<float> v{A32_.p,      xf32_lo_.p, xf32_up_.p, pkv32_lo_.p, pkv32_up_.p, dinv32_.p, inv32_cm_.p,
                          inv32_rm_.p, x_.p,       r_.p,       z_.p,        p_.p,        Ap_.p,     y_.p,
                          part_.p,     b_.p};
-        run_sweep<float>(v, true);
-        run_sweep<float>(v, false);
+        if (sweep_mode_ == 2) launch_pcg<float>(v, true, 0);
+        else {
+            run_sweep<float>(v, true);
+            run_sweep<float>(v, false);
+        }
     } else {
         if (sweep_mode_ == 0) build_windows(false);
         PcgBufs<double> v{A_.p,      xf_lo_.p, xf_up_.p, pk_val_lo_.p, pk_val_up_.p, dinv_.p, inv_cm_.p,
                           inv_rm_.p, x_.p,     r_.p,     z_.p,         p_.p,         Ap_.p,   y_.p,
                           part_.p,   b_.p};
-        run_sweep<double>(v, true);
-        run_sweep<double>(v, false);
+        if (sweep_mode_ == 2) launch_pcg<double>(v, true, 0);
+        else {
+            run_sweep<double>(v, true);
+            run_sweep<double>(v, false);
+        }
     }
     MPS_CUDA(cudaGetLastError());
     MPS_CUDA(cudaMemcpyAsync(z, z_.p, sizeof(double) * ne, cudaMemcpyDeviceToHost, st_));

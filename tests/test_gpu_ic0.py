@@ -11,9 +11,10 @@ algorithm on any numbering.  Checked through the C ABI, after one step:
     across a warp, the oracle in ascending order);
   * the in-cell block inverses (k_cell_inverse) against the oracle's
     substitution from the same factor: relative L2 <= 1e-13;
-  * one application z = (L L^T)^-1 r of the device sweeps (both sweep
-    kernels) against the oracle's triangular solves: relative L2 <= 1e-11
-    in FP64, <= 1e-4 with the mixed form's FP32 copy of the factor.
+  * one application z = (L L^T)^-1 r of the device sweeps (the persistent
+    ICCG kernel's apply mode and both launch-per-colour sweep kernels)
+    against the oracle's triangular solves: relative L2 <= 1e-11 in FP64,
+    <= 1e-4 with the mixed form's FP32 copy of the factor.
 
 Cases: a 3-D and a 2-D dam break, and a densely packed 3-D column (cells of
 up to ~90 unknowns) that reaches the sweeps' unstaged (41-64 unknowns) and
@@ -87,7 +88,7 @@ def test_factor_and_block_inverses_match_the_oracle(name, oracle3):
         assert m.max() > 64 and np.count_nonzero((m > 40) & (m <= 64)) > 0, m.max()
 
 
-@pytest.mark.parametrize("sweep", ["1", "0"])
+@pytest.mark.parametrize("sweep", ["2", "1", "0"])
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_preconditioner_apply_matches_the_oracle(name, sweep, oracle3, monkeypatch):
     _cuda()
