@@ -388,7 +388,10 @@ def run_b200(args, rank: int, world: int, local_rank: int):
                 ms_launch = pm["prof_pcg_ms"] / pm["prof_pcg_launches"]
                 ms_iter = pm["prof_pcg_ms"] / max(pm["prof_pcg_iterations"], 1)
                 b_iter = pcg_iter_bytes(pm, fp32, fp32)
-                kern[f] = {"k_pcg_ms_per_iteration": ms_iter, "k_pcg_iterations_per_launch": ipl}
+                kern[f] = {"k_pcg_ms_per_iteration": ms_iter, "k_pcg_iterations_per_launch": ipl,
+                           "spmv_phase_ms": pm["prof_spmv_ms"] / max(pm["prof_spmv_launches"], 1),
+                           "forward_phases_ms": pm["prof_fwd_ms"] / max(pm["prof_fwd_sweeps"], 1),
+                           "backward_phases_ms": pm["prof_bwd_ms"] / max(pm["prof_bwd_sweeps"], 1)}
                 t = ncu_traffic("k_pcg", f)
                 ach = b_iter / (ms_iter / 1e3) / 1e9
                 roof.append({"form": f, "kernel": "k_pcg", "bound": "hbm", "achieved": ach, "peak": peak,

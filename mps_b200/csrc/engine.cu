@@ -248,6 +248,8 @@ private:
     // k_sweep_cell over jagged-diagonal cross blocks
     int sweep_mode_ = 0;
     DevArray<unsigned> pcg_bar_;   // grid-barrier counter of k_pcg
+    DevArray<unsigned long long> pcg_trace_;    // k_pcg phase timestamps while profiling
+    std::vector<unsigned long long> trace_host_;
     int pcg_batch_ = 16;           // k_pcg iterations per launch (MPS_PCG_BATCH)
     int pcg_grid_[3] = {0, 0, 0};  // k_pcg grid per variant (FP64; FP32 difference form; FP32)
     // polls of a k_pcg grid-barrier wait (MPS_TEST_BAR_POLLS lowers it, down
@@ -362,6 +364,7 @@ private:
     template <class TM>
     void launch_pcg(const PcgBufs<TM> &v, bool apply, int batch);
     int pcg_grid(const void *kernel);
+    void trace_phases(int iterations);
     void mixed_solve(int n_eq, long long nnz, bool icc);
     void build_windows(bool fp32);
     static constexpr int kMaxUpdates = 200;      // reliable updates of the mixed form, at most
@@ -1398,6 +1401,7 @@ void Engine<D>::pcg_solve(const PcgBufs<TM> &v, double tol, int maxit, bool icc,
                 met.prof_nnz_sum += (long long)worked * nnz;
                 met.prof_rows_sum += (long long)worked * n_eq;
             }
+            if (prof) trace_phases(worked);
             iter_before = sc_host_->iter;
             if (sc_host_->done) break;
         }
@@ -1448,6 +1452,33 @@ void Engine<D>::pcg_solve(const PcgBufs<TM> &v, double tol, int maxit, bool icc,
         }
         iter_before = sc_host_->iter;
         if (sc_host_->done) break;
+    }
+}
+
+// Phase times of the last k_pcg launch from its trace (CTA 0's global timer
+// as it left each barrier), added to the profiling metrics: per iteration
+// the SpMV phase, the forward phases (the last colour's fused backward
+// in-cell product included) and the backward phases.
+template <int D>
+void Engine<D>::trace_phases(int iterations)
+{
+    int nc = 0;
+    for (int c = 0; c < (1 << D); c++) nc += act_off_[c + 1] > act_off_[c];
+    trace_host_.resize(PCG_TRACE + 2);
+    MPS_CUDA(cudaMemcpy(trace_host_.data(), pcg_trace_.p, sizeof(unsigned long long) * (PCG_TRACE + 2),
+                        cudaMemcpyDeviceToHost));
+    long long nbar = (long long)trace_host_[PCG_TRACE + 1];
+    const unsigned long long *t = trace_host_.data();
+    int per = 2 * nc;   // barriers per iteration
+    for (int it = 0; it < iterations; it++) {
+        long long b0 = (long long)it * per;
+        if (b0 + per > nbar || b0 + per > PCG_TRACE) break;
+        met.prof_spmv_ms += 1e-6 * (double)(t[b0 + 1] - t[b0]);
+        met.prof_spmv_launches += 1;
+        met.prof_fwd_ms += 1e-6 * (double)(t[b0 + 1 + nc] - t[b0 + 1]);
+        met.prof_fwd_sweeps += 1;
+        met.prof_bwd_ms += 1e-6 * (double)(t[b0 + per] - t[b0 + 1 + nc]);
+        met.prof_bwd_sweeps += 1;
     }
 }
 
@@ -1521,6 +1552,11 @@ void Engine<D>::launch_pcg(const PcgBufs<TM> &v, bool apply, int batch)
     a.batch = batch;
     a.apply = apply ? 1 : 0;
     a.bar_polls = bar_polls_;
+    a.trace = nullptr;
+    if (profiling && !apply) {
+        pcg_trace_.reserve(PCG_TRACE + 2);
+        a.trace = pcg_trace_.p;
+    }
     const void *k;
     int variant;
     if constexpr (sizeof(TM) == 8) {

@@ -72,7 +72,20 @@ struct PcgArgs {
     int batch;                 // iterations in this launch, at most
     int apply;                 // 1: only z = M^-1 r (both sweeps), no CG update
     int bar_polls;             // polls of one grid-barrier wait, at most
+    // profiling: CTA 0 writes the global timer at its start (trace[0]) and as
+    // it leaves barrier k (trace[k], k <= PCG_TRACE), and the number of
+    // barriers passed at trace[PCG_TRACE + 1]; null when off
+    unsigned long long *trace;
 };
+
+constexpr int PCG_TRACE = 4096;
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p)
 {
@@ -401,10 +414,21 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs<TM> a)
     const unsigned G = gridDim.x;
     unsigned nbar = 0;
     int nsum = 0;
-    auto barrier = [&]() { return grid_barrier(a.bar, ++nbar * G, a.bar_polls, a.err, &s_ok); };
+    const bool tr = a.trace && blockIdx.x == 0 && threadIdx.x == 0;
+    if (tr) a.trace[0] = global_ns();
+    auto mark = [&]() {
+        if (tr && nbar <= PCG_TRACE) a.trace[nbar] = global_ns();
+    };
+    auto barrier = [&]() {
+        bool ok = grid_barrier(a.bar, ++nbar * G, a.bar_polls, a.err, &s_ok);
+        mark();
+        return ok;
+    };
     auto gsum = [&](double v, double *out) {
-        return grid_sum(v, a.partials, (nsum++) % PCG_SLOTS, a.bar, ++nbar * G, a.bar_polls, a.err, s_red, &s_ok,
-                        out);
+        bool ok = grid_sum(v, a.partials, (nsum++) % PCG_SLOTS, a.bar, ++nbar * G, a.bar_polls, a.err, s_red,
+                           &s_ok, out);
+        mark();
+        return ok;
     };
     const int nc = a.ncol;
     double arr = 0.0, arz = 0.0;
@@ -482,6 +506,7 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs<TM> a)
         for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n_eq; i += gridDim.x * blockDim.x)
             a.p[i] = pend ? a.z[i] + beta * pold[i] : pold[i];
     }
+    if (tr) a.trace[PCG_TRACE + 1] = nbar;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         sc->rz = rz;
         sc->rr = rr;
