@@ -255,6 +255,9 @@ private:
     // polls of a k_pcg grid-barrier wait (MPS_TEST_BAR_POLLS lowers it, down
     // to 0, to exercise the timeout path)
     int bar_polls_ = PCG_BAR_POLLS;
+    // entries per lane loaded in one batch by k_sweep_colour's head sums
+    // (MPS_SWEEP_HB: 4 or 8)
+    int head_batch_ = 4;
     // polls of the first wait for a staged block inverse (MPS_TEST_MBAR_POLLS
     // lowers it, down to 0, to exercise the timeout path)
     int first_polls_ = MBAR_POLLS;
@@ -411,6 +414,7 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
         int v = std::atoi(e);
         sweep_mode_ = (v == 0 || v == 1) ? v : 2;
     }
+    if (const char *e = std::getenv("MPS_SWEEP_HB")) head_batch_ = std::atoi(e) == 8 ? 8 : 4;
     if (const char *e = std::getenv("MPS_PCG_BATCH")) {
         int v = std::atoi(e);
         if (v >= 1 && v <= 1024) pcg_batch_ = v;
@@ -443,6 +447,10 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
     MPS_CUDA(cudaFuncSetAttribute(k_sweep_colour<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(sizeof(double) * CELL_STAGE_MAX)));
     MPS_CUDA(cudaFuncSetAttribute(k_sweep_colour<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(double) * CELL_STAGE_MAX)));
+    MPS_CUDA(cudaFuncSetAttribute(k_sweep_colour<true, double, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(double) * CELL_STAGE_MAX)));
+    MPS_CUDA(cudaFuncSetAttribute(k_sweep_colour<false, double, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(sizeof(double) * CELL_STAGE_MAX)));
     alloc_state();
     build_grid();
@@ -1295,6 +1303,7 @@ void Engine<D>::run_sweep(const PcgBufs<TM> &v, bool fwdir)
             return;
         }
         auto colk = fwdir ? k_sweep_colour<true, TM> : k_sweep_colour<false, TM>;
+        if (head_batch_ == 8) colk = fwdir ? k_sweep_colour<true, TM, 8> : k_sweep_colour<false, TM, 8>;
         for (int i = 0; i < nc; i++) {
             int c = order[i], cn = i + 1 < nc ? order[i + 1] : -1;
             int nrb = cn >= 0 ? row_off_[cn] : 0, nre = cn >= 0 ? row_off_[cn + 1] : 0;

@@ -732,7 +732,7 @@ __global__ void k_gather_colour_offsets(ColourIdx at, int n, const int *__restri
 // dependent: what it loads before pdl_wait() (row bounds, factor values and
 // columns, block inverses, cell descriptors) is written once per step,
 // before the CG loop; x, part and the CG scalars are read only after it.
-template <bool FWD, class TM>
+template <bool FWD, class TM, int HB = 4>
 __global__ void __launch_bounds__(CELL_THREADS, 6)
 k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict__ desc,
                const int *__restrict__ inv_off, const TM *__restrict__ inv, const int *__restrict__ pk_off,
@@ -756,10 +756,11 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
             a = FWD ? __ldg(&xp[r]) : __ldg(&xs[r]);
             b = FWD ? __ldg(&xs[r]) : __ldg(&xp[r + 1]);
         }
-        TM f[4];
-        int cc[4];
+        // the first HB entries of each lane in one batch, before the wait
+        TM f[HB];
+        int cc[HB];
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
+        for (int u = 0; u < HB; u++) {
             int q = a + lane + u * LPR;
             bool ok = q < b;
             f[u] = ok ? __ldg(&xf[q]) : TM(0);
@@ -769,9 +770,9 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
         if (sc->done) return;
         T s = T(0);
 #pragma unroll
-        for (int u = 0; u < 4; u++)
+        for (int u = 0; u < HB; u++)
             if (cc[u] >= 0) s += T(f[u]) * x[cc[u]];
-        for (int q = a + lane + 4 * LPR; q < b; q += LPR) s += T(__ldg(&xf[q])) * x[__ldg(&xc[q])];
+        for (int q = a + lane + HB * LPR; q < b; q += LPR) s += T(__ldg(&xf[q])) * x[__ldg(&xc[q])];
 #pragma unroll
         for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LPR);
         if (lane == 0 && r < nre) part[r] = rhs[r] - s;
@@ -810,7 +811,21 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
             if (r < R1) {
                 int a = FWD ? __ldg(&xs[r]) : __ldg(&xp[r]);
                 int e = FWD ? __ldg(&xp[r + 1]) : __ldg(&xs[r]);
-                for (int q = a + lane; q < e; q += TL) s += T(__ldg(&xf[q])) * x[__ldg(&xc[q])];
+                // the first TB entries of each lane in one batch of loads
+                constexpr int TB = 4;
+                TM tf[TB];
+                int tc[TB];
+#pragma unroll
+                for (int u = 0; u < TB; u++) {
+                    int q = a + lane + u * TL;
+                    bool ok = q < e;
+                    tf[u] = ok ? __ldg(&xf[q]) : TM(0);
+                    tc[u] = ok ? __ldg(&xc[q]) : -1;
+                }
+#pragma unroll
+                for (int u = 0; u < TB; u++)
+                    if (tc[u] >= 0) s += T(tf[u]) * x[tc[u]];
+                for (int q = a + lane + TB * TL; q < e; q += TL) s += T(__ldg(&xf[q])) * x[__ldg(&xc[q])];
             }
             s += __shfl_down_sync(0xffffffffu, s, 1, TL);
             if (lane == 0 && r < R1) part[r] = (first ? rhs[r] : part[r]) - s;
