@@ -1313,7 +1313,7 @@ void Engine<D>::run_sweep(const PcgBufs<TM> &v, bool fwdir)
                fwdir ? v.inv_cm : v.inv_rm, pko, pkl, pkv, pkk, v.dinv, (const int *)(fwdir ? xp_lo_.p : xp_up_.p),
                (const int *)(fwdir ? xs_lo_.p : xs_up_.p), (const int *)(fwdir ? xc_lo_.p : xc_up_.p),
                fwdir ? v.xf_lo : v.xf_up, (int)(i == 0), nrb, nre, rhs, v.part, out, (const CGScalars *)sc_.p,
-               win_ + CELL_MAXBLK, err_.p);
+               win_ + CELL_MAXBLK, first_polls_, err_.p);
         }
     }
 }

@@ -665,6 +665,22 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, int lim
 }
 
 constexpr int MBAR_POLLS = 1 << 20;
+constexpr int MBAR_DRAIN_POLLS = 1 << 26;
+
+// Bounded wait for a warp's bulk copy: false (and ERR_COPY_TIMEOUT set)
+// after `polls` polls, in which case the copy is first waited for with the
+// long bound, so that the warp never leaves it in flight.
+__device__ __forceinline__ bool stage_wait(unsigned bar, int polls, unsigned *err)
+{
+    if (mbar_wait(bar, 0, polls)) return true;
+    atomicOr(err, ERR_COPY_TIMEOUT);
+    for (int i = 0; i < MBAR_DRAIN_POLLS; i++) {
+        if (mbar_wait(bar, 0, 1)) break;
+        __nanosleep(64);
+    }
+    return false;
+}
+
 
 // ---- staged in-cell sweep -----------------------------------------------------
 //
@@ -739,7 +755,7 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
                const int *__restrict__ pk_len, const TM *__restrict__ pk_val, const unsigned char *__restrict__ pk_k,
                const TM *__restrict__ dinv, const int *__restrict__ xp, const int *__restrict__ xs,
                const int *__restrict__ xc, const TM *__restrict__ xf, int first, int nrb, int nre, const double *rhs,
-               double *part, double *x, const CGScalars *sc, int stage_elems, unsigned *err)
+               double *part, double *x, const CGScalars *sc, int stage_elems, int first_polls, unsigned *err)
 {
     using T = double;   // vectors and sums; TM is the storage type of the factor
     constexpr int LPR = 8;
@@ -832,11 +848,8 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
         }
     }
     __syncthreads();
-    if (staged && !mbar_wait(b, 0, MBAR_POLLS)) {
-        if (threadIdx.x == 0) atomicOr(err, ERR_COPY_TIMEOUT);
-        mbar_wait(b, 0, MBAR_POLLS);
-        return;
-    }
+    // on a timeout the copy is still waited for (long bound) before the CTA returns
+    if (staged && !stage_wait(b, first_polls, err)) return;
     if (nel > stage_elems && threadIdx.x == 0) atomicOr(err, ERR_WINDOW_OVERFLOW);
     if (done) return;
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -930,7 +943,6 @@ constexpr int JSTAGE_M = 40;          // cells of up to this many unknowns stage
 constexpr int JSTAGE = ((JSTAGE_M * (JSTAGE_M + 1) / 2) + 3) & ~3;
 constexpr int JU = 4;                 // diagonals per warp loaded in one batch
 constexpr int JMAXL = 512;            // cross entries of one row, at most (the list's max_neighbors bound)
-constexpr int MBAR_DRAIN_POLLS = 1 << 26;
 
 // Diagonals of every active cell's jagged-diagonal block: 1 + the longest
 // cross run among its rows (xp: the runs' offsets in row order).
@@ -1011,20 +1023,6 @@ k_jds_fill(int nact, const int2 *__restrict__ desc, const int *__restrict__ xp, 
             xf[dst] = F[src + k];
         }
     }
-}
-
-// Bounded wait for a warp's bulk copy: false (and ERR_COPY_TIMEOUT set)
-// after `polls` polls, in which case the copy is first waited for with the
-// long bound, so that the warp never leaves it in flight.
-__device__ __forceinline__ bool stage_wait(unsigned bar, int polls, unsigned *err)
-{
-    if (mbar_wait(bar, 0, polls)) return true;
-    atomicOr(err, ERR_COPY_TIMEOUT);
-    for (int i = 0; i < MBAR_DRAIN_POLLS; i++) {
-        if (mbar_wait(bar, 0, 1)) break;
-        __nanosleep(64);
-    }
-    return false;
 }
 
 template <bool FWD, class TM>
