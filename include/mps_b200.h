@@ -70,7 +70,8 @@ typedef struct {
     double surface_count_threshold;
     double restitution_coeff;
     double collision_distance_ratio;
-    int    surface_tension_enabled;   /* must be 0: not on this path */
+    int    surface_tension_enabled;   /* potential-force surface tension (operators.c:281-354); its
+                                         radius, coefficient and contact angle are at the end */
     double domain_min[3];
     double domain_max[3];
     int    cmps_gradient;
@@ -89,6 +90,13 @@ typedef struct {
     double wall_drive_amp;            /* A (m) */
     double wall_drive_freq;           /* f (Hz) */
     int    wall_drive_axis;           /* 0 = x, 1 = y, 2 = z */
+    /* Surface tension (sim_config.h: influence_radius_st = re_ratio * l0,
+     * surface_tension_coeff sigma, wetting_angle_SL theta in degrees); read
+     * only when surface_tension_enabled.  The list radius then includes
+     * influence_radius_st, as simulation.c:22-24 does. */
+    double influence_radius_st;
+    double surface_tension_coeff;
+    double wetting_angle_SL;
 } mps_params_t;
 
 /* Per-step metrics (the reference computes and discards its iteration count,
@@ -239,6 +247,13 @@ int  mps_get_metrics(mps_session *s, mps_metrics_t *m);
 /* Kernels launched by this library in this process so far. */
 unsigned long long mps_launch_count(void);
 
+/* The surface-tension coefficients the reference calibrates in
+ * particle_system_calc_initial_params (particle.c:185-211, 2-D
+ * particle.c:154-180): C_LL from the potential's interaction energy across a
+ * flat interface of the rest lattice, C_SL = (1 + cos theta) / 2 C_LL.  Both
+ * 0 when surface tension is off.  Host arithmetic, no device needed. */
+int  mps_surface_tension_coeffs(const mps_params_t *params, double *c_ll, double *c_sl);
+
 /* Per-kernel timing of the CG loop with CUDA events (adds no host sync). */
 int  mps_set_profiling(mps_session *s, int on);
 /* Zero the accumulated metrics. */
@@ -262,6 +277,8 @@ void *mps_get_stream(mps_session *s);
 #define MPS_STAGE_WALL           9   /* apply_wall_boundary           (boundary.c:12) */
 #define MPS_STAGE_OUT_OF_BOUNDS 10   /* remove_out_of_bounds          (boundary.c:33) */
 #define MPS_STAGE_SURFACE_BY_COUNT 11 /* judge_free_surface_by_count (operators.c:253); arg = beta */
+#define MPS_STAGE_SURFACE_TENSION 12  /* calc_surface_tension      (operators.c:281) */
+#define MPS_STAGE_SURFACE_TENSION_SL 13 /* calc_surface_tension_SL (operators.c:322) */
 int  mps_run_stage(mps_session *s, int stage, const int *neighbors, const int *count,
                    int max_nb, double arg);
 

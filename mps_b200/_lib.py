@@ -35,6 +35,8 @@ STAGES = {
     "wall": 9,
     "out_of_bounds": 10,
     "surface_by_count": 11,
+    "surface_tension": 12,
+    "surface_tension_sl": 13,
 }
 
 
@@ -74,6 +76,9 @@ class MpsParams(C.Structure):
         ("wall_drive_amp", C.c_double),
         ("wall_drive_freq", C.c_double),
         ("wall_drive_axis", C.c_int),
+        ("influence_radius_st", C.c_double),
+        ("surface_tension_coeff", C.c_double),
+        ("wetting_angle_SL", C.c_double),
     ]
 
 
@@ -156,6 +161,7 @@ SIGNATURES = {
     "mps_get_metrics": (I, [P, C.POINTER(MpsMetrics)]),
     "mps_get_stream": (P, [P]),
     "mps_launch_count": (C.c_ulonglong, []),
+    "mps_surface_tension_coeffs": (I, [C.POINTER(MpsParams), DP, DP]),
     "mps_set_profiling": (I, [P, I]),
     "mps_reset_metrics": (I, [P]),
     "mps_run_stage": (I, [P, I, P, P, I, C.c_double]),
@@ -206,7 +212,8 @@ def params_from_config(cfg, dim: int, precision: int = PREC_FP64, refine_toleran
               "relaxation_coeff", "clamp_negative_pressure", "ppe_type", "c_ppe", "gamma_ppe",
               "surface_threshold", "surface_detection_method", "surface_count_threshold",
               "restitution_coeff", "collision_distance_ratio", "surface_tension_enabled",
-              "cmps_gradient", "use_analytical_lambda", "hs_mode"):
+              "cmps_gradient", "use_analytical_lambda", "hs_mode", "influence_radius_st",
+              "surface_tension_coeff", "wetting_angle_SL"):
         setattr(p, f, getattr(cfg, f))
     for d in range(dim):
         p.gravity[d] = cfg.gravity[d]

@@ -118,6 +118,9 @@ struct Consts {
     int    ppe_type, hs_mode, cmps, surf_method, clamp;
     int    collision_on;
     int    drive_on, drive_axis;   // driven walls (A != 0) and their axis
+    int    st_on, st_sl_on;        // surface tension; its wall term (C_SL != 0)
+    double st_ll, st_sl;           // C_LL / (rho l0^D), C_SL / (rho l0^D)   operators.c:284, :326
+    double re_st, st_rmin;         // influence_radius_st, 1e-9 * l0          operators.c:303
 };
 
 // Structure-of-arrays particle state.  `key` holds the positions at the

@@ -92,6 +92,9 @@ mps_params_t params_from(const SimConfig *c)
     p.restitution_coeff = c->restitution_coeff;
     p.collision_distance_ratio = c->collision_distance_ratio;
     p.surface_tension_enabled = c->surface_tension_enabled;
+    p.influence_radius_st = c->influence_radius_st;
+    p.surface_tension_coeff = c->surface_tension_coeff;
+    p.wetting_angle_SL = c->wetting_angle_SL;
     p.cmps_gradient = c->cmps_gradient;
     p.use_analytical_lambda = c->use_analytical_lambda;
     p.hs_mode = c->hs_mode;
@@ -494,10 +497,6 @@ int particle_system_add(ParticleSystem *ps, double pos[], double vel[], int type
 
 void particle_system_calc_initial_params(ParticleSystem *ps)
 {
-    if (g_config && g_config->surface_tension_enabled) {
-        fail("particle_system_calc_initial_params", MPS_ERR_UNSUPPORTED, nullptr);
-        return;
-    }
     Ctx *c = ctx_for(ps);
     if (!c || !upload(c, ps, false)) return;
     double n0 = 0, lam = 0;
@@ -506,9 +505,16 @@ void particle_system_calc_initial_params(ParticleSystem *ps)
     ps->n0 = n0;
     ps->lambda = lam;
     if (g_config->surface_detection_method == 1) ps->n0_count = n0c;
+    if (g_config->surface_tension_enabled) {
+        mps_params_t p = params_from(g_config);
+        mps_surface_tension_coeffs(&p, &ps->C_LL, &ps->C_SL);
+    }
     std::printf("Initial params: n0 = %.6f (re_n=%.4f)  N0 = %d  lambda = %.6f (re_lap=%.4f)%s\n", ps->n0,
                 g_config->influence_radius_n, ps->n0_count, ps->lambda, g_config->influence_radius_lap,
                 g_config->use_analytical_lambda ? "  [analytical]" : "");
+    if (g_config->surface_tension_enabled)
+        std::printf("  C_LL = %.6e  C_SL = %.6e (theta=%.1f deg, re_st=%.4f)\n", ps->C_LL, ps->C_SL,
+                    g_config->wetting_angle_SL, g_config->influence_radius_st);
 }
 
 // ---- kernel function (kernel.c:12-30) -------------------------------------------
@@ -677,18 +683,17 @@ void collision(ParticleSystem *ps, NeighborList *nl) { stage(ps, nl, MPS_STAGE_C
 void collision(ParticleSystem *ps) { stage(ps, nullptr, MPS_STAGE_COLLISION, 0.0, false, "collision"); }
 #endif
 
+// The coefficients come from the caller's particle system (ps->C_LL,
+// ps->C_SL), as the reference's functions read them.
 void calc_surface_tension(ParticleSystem *ps, NeighborList *nl)
 {
-    (void)ps;
-    (void)nl;
-    fail("calc_surface_tension (surface tension is not on this path)", MPS_ERR_UNSUPPORTED, nullptr);
+    stage(ps, nl, MPS_STAGE_SURFACE_TENSION, ps->C_LL, false, "calc_surface_tension");
 }
 
 void calc_surface_tension_SL(ParticleSystem *ps, NeighborList *nl)
 {
-    (void)ps;
-    (void)nl;
-    fail("calc_surface_tension_SL (surface tension is not on this path)", MPS_ERR_UNSUPPORTED, nullptr);
+    if (ps->C_SL == 0.0) return;
+    stage(ps, nl, MPS_STAGE_SURFACE_TENSION_SL, ps->C_SL, false, "calc_surface_tension_SL");
 }
 
 void solve_pressure(ParticleSystem *ps, NeighborList *nl)

@@ -37,6 +37,49 @@ namespace mps {
 
 static inline int nblk(long long n, int b) { return (int)((n + b - 1) / b); }
 
+// The neighbour-list radius (simulation.c:22-24): the largest active radius.
+static double list_radius(const mps_params_t &p)
+{
+    double re = std::fmax(p.influence_radius_lap, p.influence_radius_n);
+    if (p.surface_tension_enabled) re = std::fmax(re, p.influence_radius_st);
+    return re;
+}
+
+// Surface-tension coefficients of particle.c:185-211 (2-D particle.c:154-180):
+// the potential's interaction energy summed over lattice pairs across a flat
+// interface, C_LL = sigma l0^(D-1) / sum, C_SL = (1 + cos theta) / 2 C_LL;
+// the same expressions in the same order, so the values are the reference's.
+static void surface_tension_coeffs(const mps_params_t &p, double *cll, double *csl)
+{
+    *cll = 0.0;
+    *csl = 0.0;
+    if (!p.surface_tension_enabled) return;
+    double l0 = p.particle_distance, re_st = p.influence_radius_st;
+    int nmax = (int)std::ceil(re_st / l0);
+    double sum = 0.0;
+    for (int dxa = 1; dxa <= nmax; dxa++)
+        for (int dxb = -(nmax - 1); dxb <= 0; dxb++)
+            for (int dyb = -nmax; dyb <= nmax; dyb++)
+                for (int dzb = (p.dim == 3 ? -nmax : 0); dzb <= (p.dim == 3 ? nmax : 0); dzb++) {
+                    double rx = (double)(dxa - dxb) * l0;
+                    double ry = (double)dyb * l0;
+                    double rab;
+                    if (p.dim == 3) {
+                        double rz = (double)dzb * l0;
+                        rab = std::sqrt(rx * rx + ry * ry + rz * rz);
+                    } else {
+                        rab = std::sqrt(rx * rx + ry * ry);
+                    }
+                    if (rab > 0.0 && rab < re_st)
+                        sum += (1.0 / 3.0) * (rab - 1.5 * l0 + 0.5 * re_st) * (rab - re_st) * (rab - re_st);
+                }
+    if (sum > 0.0) {
+        *cll = (p.dim == 3) ? p.surface_tension_coeff * l0 * l0 / sum : p.surface_tension_coeff * l0 / sum;
+        double theta = p.wetting_angle_SL * M_PI / 180.0;
+        *csl = 0.5 * (1.0 + std::cos(theta)) * *cll;
+    }
+}
+
 constexpr int TPB = 256;             // threads per block, particle kernels
 constexpr int RED_BLOCKS = 148 * 8;  // fixed grid of the reduction kernels: full occupancy at 256 threads
 constexpr int CG_BATCH = 8;          // CG iterations between convergence reads
@@ -396,7 +439,6 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
 {
     if (p.dim != D) throw CudaError("dimension mismatch", MPS_ERR_INVALID);
     if (capacity <= 0) throw CudaError("capacity must be positive", MPS_ERR_INVALID);
-    if (p.surface_tension_enabled) throw CudaError("surface tension is not on this path", MPS_ERR_UNSUPPORTED);
     if (p.wall_drive_axis < 0 || p.wall_drive_axis >= D) throw CudaError("wall_drive_axis out of range", MPS_ERR_INVALID);
     cap_ = capacity;
     prm_ = p;
@@ -550,7 +592,7 @@ void Engine<D>::alloc_state()
 template <int D>
 void Engine<D>::build_grid()
 {
-    double re = std::fmax(prm_.influence_radius_lap, prm_.influence_radius_n);
+    double re = list_radius(prm_);
     re_list_ = re;
     double margin = 4.0 * re;
     long long total = 1;
@@ -651,18 +693,27 @@ void Engine<D>::compute_consts()
     k.collision_on = (D == 2) ? 1 : (p.collision_distance_ratio > 0.0);
     k.drive_on = p.wall_drive_amp != 0.0;
     k.drive_axis = p.wall_drive_axis;
+    // surface tension (operators.c:283-285, 2-D :233-235): coeff = C / (rho l0^D)
+    k.st_on = p.surface_tension_enabled != 0;
+    double cll = 0.0, csl = 0.0;
+    surface_tension_coeffs(p, &cll, &csl);
+    double l0 = p.particle_distance;
+    k.st_ll = (D == 3) ? cll / (p.density * l0 * l0 * l0) : cll / (p.density * l0 * l0);
+    k.st_sl = (D == 3) ? csl / (p.density * l0 * l0 * l0) : csl / (p.density * l0 * l0);
+    k.st_sl_on = csl != 0.0;
+    k.re_st = p.influence_radius_st;
+    k.st_rmin = 1.0e-9 * l0;
 }
 
 template <int D>
 void Engine<D>::update_params(const mps_params_t &p)
 {
     if (p.dim != D) throw CudaError("dimension mismatch", MPS_ERR_INVALID);
-    if (p.surface_tension_enabled) throw CudaError("surface tension is not on this path", MPS_ERR_UNSUPPORTED);
     if (p.wall_drive_axis < 0 || p.wall_drive_axis >= D) throw CudaError("wall_drive_axis out of range", MPS_ERR_INVALID);
     bool regrid = false;
     for (int d = 0; d < D; d++)
         regrid |= p.domain_min[d] != prm_.domain_min[d] || p.domain_max[d] != prm_.domain_max[d];
-    regrid |= std::fmax(p.influence_radius_lap, p.influence_radius_n) != re_list_;
+    regrid |= list_radius(p) != re_list_;
     prm_ = p;
     if (regrid) {
         build_grid();
@@ -970,6 +1021,10 @@ void Engine<D>::explicit_stage(bool from_list)
     int nb = nblk(n, TPB);
     if (from_list) launch(k_viscosity<D, ListSource>, nb, TPB, 0, st_, list(), S(), k_, n, 0);
     else launch(k_viscosity<D, CellSource<D>>, nb, TPB, 0, st_, cells(), S(), k_, n, 0);
+    if (k_.st_on) {
+        if (from_list) launch(k_surface_tension<D, ListSource>, nb, TPB, 0, st_, list(), S(), k_, n, 3);
+        else launch(k_surface_tension<D, CellSource<D>>, nb, TPB, 0, st_, cells(), S(), k_, n, 3);
+    }
     launch(k_explicit_update<D>, nb, TPB, 0, st_, S(), k_, n);
     if (k_.drive_on) {
         double dx, vel;
@@ -2193,6 +2248,7 @@ void Engine<D>::run_stage(int stage, const int *nb, const int *cnt, int max_nb, 
     int n = n_;
     bool needs_list = stage == MPS_STAGE_DENSITY || stage == MPS_STAGE_VISCOSITY || stage == MPS_STAGE_GRADIENT ||
                       stage == MPS_STAGE_NEIGHBOR_COUNT || stage == MPS_STAGE_SOLVE_PRESSURE ||
+                      stage == MPS_STAGE_SURFACE_TENSION || stage == MPS_STAGE_SURFACE_TENSION_SL ||
                       (stage == MPS_STAGE_COLLISION && D == 3);
     bool needs_ref = stage == MPS_STAGE_VISCOSITY || stage == MPS_STAGE_GRADIENT ||
                      stage == MPS_STAGE_SOLVE_PRESSURE || stage == MPS_STAGE_SURFACE ||
@@ -2244,6 +2300,21 @@ void Engine<D>::run_stage(int stage, const int *nb, const int *cnt, int max_nb, 
         if (by_count) k.count_thr = arg * n0_count_;
         else k.surf_thr = arg * n0_;
         launch(k_surface<D>, bl, TPB, 0, st_, S(), k, n, by_count);
+        break;
+    }
+    case MPS_STAGE_SURFACE_TENSION:
+    case MPS_STAGE_SURFACE_TENSION_SL: {
+        // arg = C_LL or C_SL of the caller's particle system (operators.c:284, :326)
+        Consts k = k_;
+        double l0 = prm_.particle_distance;
+        double c = (D == 3) ? arg / (prm_.density * l0 * l0 * l0) : arg / (prm_.density * l0 * l0);
+        int which = stage == MPS_STAGE_SURFACE_TENSION ? 1 : 2;
+        if (which == 1) k.st_ll = c;
+        else {
+            k.st_sl = c;
+            k.st_sl_on = arg != 0.0;
+        }
+        launch(k_surface_tension<D, ListSource>, bl, TPB, 0, st_, list(), S(), k, n, which);
         break;
     }
     case MPS_STAGE_CLAMP:
@@ -2454,6 +2525,13 @@ void *mps_get_stream(mps_session *s) { return (s && s->eng) ? (void *)s->eng->st
 const char *mps_last_error(mps_session *s)
 {
     return (s && s->eng) ? s->eng->last_error.c_str() : "no session";
+}
+
+int mps_surface_tension_coeffs(const mps_params_t *params, double *c_ll, double *c_sl)
+{
+    if (!params || !c_ll || !c_sl) return MPS_ERR_INVALID;
+    mps::surface_tension_coeffs(*params, c_ll, c_sl);
+    return MPS_OK;
 }
 
 int mps_run_stage(mps_session *s, int stage, const int *neighbors, const int *count, int max_nb, double arg)

@@ -53,6 +53,42 @@ __global__ void k_viscosity(Src src, State<D> s, Consts k, int n, int accumulate
     }
 }
 
+// Surface tension of the potential model (operators.c:281-354, 2-D
+// operators.c:231-309), added to the acceleration of every fluid particle:
+// first the fluid neighbours (liquid-liquid, coefficient ll = C_LL / (rho
+// l0^D)), then, when `sl_on`, the wall neighbours (solid-liquid, sl), each in
+// list order, for pairs with 1e-9 l0 <= r < re_st:
+//   acc += (coeff * f) * (dr / r),  f = -(r - l0) (r - re_st).
+// which: 1 the fluid pass, 2 the wall pass, 3 both (the step).
+template <int D, class Src>
+__global__ void k_surface_tension(Src src, State<D> s, Consts k, int n, int which)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || s.type[i] != FLUID) return;
+    double pi[D], a[D];
+    load_vec<D>(pi, s.pos, i);
+    load_vec<D>(a, s.acc, i);
+    for (int pass = 0; pass < 2; pass++) {
+        if (!(which & (1 << pass))) continue;
+        if (pass == 1 && !k.st_sl_on) continue;
+        int want = pass == 0 ? FLUID : WALL;
+        double coeff = pass == 0 ? k.st_ll : k.st_sl;
+        src.for_each(i, [&](int j) {
+            if (s.type[j] != want) return;
+            double pj[D], dr[D];
+            load_vec<D>(pj, s.pos, j);
+            double r = sqrt(dist2v<D>(pi, pj, dr));
+            if (r < k.st_rmin || r >= k.re_st) return;
+            double f = -(r - k.l0) * (r - k.re_st);
+            double cf = coeff * f;
+#pragma unroll
+            for (int d = 0; d < D; d++) a[d] += cf * (dr[d] / r);
+        });
+    }
+#pragma unroll
+    for (int d = 0; d < D; d++) s.acc[d][i] = a[d];
+}
+
 template <int D>
 __global__ void k_explicit_update(State<D> s, Consts k, int n)
 {

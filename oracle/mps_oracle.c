@@ -82,6 +82,46 @@ static void finish_initial_params(ParticleSystem *ps, const SimConfig *cfg, int 
         ps->lambda = (best_den > 1.0e-10) ? best_num / best_den : 1.0;
 }
 
+/* Surface-tension coefficients, 3P particle.c:185-211 (2D particle.c:154-180):
+ * the potential's interaction energy summed over rest-lattice pairs across a
+ * flat interface; C_LL = sigma l0^(D-1) / sum, C_SL = (1 + cos theta) / 2 C_LL. */
+static void surface_tension_coeffs(ParticleSystem *ps, const SimConfig *cfg)
+{
+    if (!cfg->surface_tension_enabled) return;
+    double l0 = cfg->particle_distance, re_st = cfg->influence_radius_st;
+    int nmax = (int)ceil(re_st / l0);
+    double sum = 0.0;
+    for (int dxa = 1; dxa <= nmax; dxa++)
+        for (int dxb = -(nmax - 1); dxb <= 0; dxb++)
+            for (int dyb = -nmax; dyb <= nmax; dyb++) {
+#if D == 3
+                for (int dzb = -nmax; dzb <= nmax; dzb++) {
+                    double rx = (double)(dxa - dxb) * l0;
+                    double ry = (double)dyb * l0;
+                    double rz = (double)dzb * l0;
+                    double rab = sqrt(rx * rx + ry * ry + rz * rz);
+                    if (rab > 0.0 && rab < re_st)
+                        sum += (1.0 / 3.0) * (rab - 1.5 * l0 + 0.5 * re_st) * (rab - re_st) * (rab - re_st);
+                }
+#else
+                double rx = (double)(dxa - dxb) * l0;
+                double ry = (double)dyb * l0;
+                double rab = sqrt(rx * rx + ry * ry);
+                if (rab > 0.0 && rab < re_st)
+                    sum += (1.0 / 3.0) * (rab - 1.5 * l0 + 0.5 * re_st) * (rab - re_st) * (rab - re_st);
+#endif
+            }
+    if (sum > 0.0) {
+#if D == 3
+        ps->C_LL = cfg->surface_tension_coeff * l0 * l0 / sum;
+#else
+        ps->C_LL = cfg->surface_tension_coeff * l0 / sum;
+#endif
+        double theta = cfg->wetting_angle_SL * M_PI / 180.0;
+        ps->C_SL = 0.5 * (1.0 + cos(theta)) * ps->C_LL;
+    }
+}
+
 static int initial_count_for(const ParticleSystem *ps, int i, double re_n2)
 {
     int c = 0;
@@ -126,6 +166,7 @@ void oracle_calc_initial_params(ParticleSystem *ps, const SimConfig *cfg)
         }
         ps->n0_count = best;
     }
+    surface_tension_coeffs(ps, cfg);
 }
 
 /* Same result bit for bit, O(N*K) instead of O(N^2): candidates come from a
@@ -247,6 +288,7 @@ void oracle_calc_initial_params_cells(ParticleSystem *ps, const SimConfig *cfg)
     }
     finish_initial_params(ps, cfg, found, best_n0, best_num, best_den);
     if (found && cfg->surface_detection_method == 1) ps->n0_count = best_cnt;
+    if (found) surface_tension_coeffs(ps, cfg);
     free(cand); free(cell_of); free(start); free(order);
 }
 
@@ -385,6 +427,46 @@ void oracle_number_density(ParticleSystem *ps, const NeighborList *nl, const Sim
 }
 
 /* 3P operators.c:50-85: acc += (nu * 2d/(n0 lambda)) * sum (u_j - u_i) w */
+/* Surface tension, 3P operators.c:281-354 (2D operators.c:231-309): the
+ * potential force f(r) = -(r - l0)(r - re_st) of the fluid neighbours (C_LL)
+ * and, unless C_SL is 0, of the wall neighbours (C_SL), on fluid particles,
+ * coeff = C / (rho l0^D), acc += coeff * f * (dr / r) in list order. */
+static void surface_tension_pass(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg, double C,
+                                 int partner)
+{
+    double re_st = cfg->influence_radius_st;
+    double l0 = cfg->particle_distance;
+#if D == 3
+    double coeff = C / (cfg->density * l0 * l0 * l0);
+#else
+    double coeff = C / (cfg->density * l0 * l0);
+#endif
+    for (int i = 0; i < ps->num; i++) {
+        Particle *pi = &ps->particles[i];
+        if (pi->type != MPS_FLUID) continue;
+        for (int k = 0; k < nl->count[i]; k++) {
+            int j = NB(nl, i, k);
+            if (ps->particles[j].type != partner) continue;
+            double dr[D];
+            double r = sqrt(dist2_vec(pi->pos, ps->particles[j].pos, dr));
+            if (r < 1.0e-9 * l0 || r >= re_st) continue;
+            double force_mag = -(r - l0) * (r - re_st);
+            for (int d = 0; d < D; d++) pi->acc[d] += coeff * force_mag * (dr[d] / r);
+        }
+    }
+}
+
+void oracle_surface_tension(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg)
+{
+    surface_tension_pass(ps, nl, cfg, ps->C_LL, MPS_FLUID);
+}
+
+void oracle_surface_tension_SL(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg)
+{
+    if (ps->C_SL == 0.0) return;
+    surface_tension_pass(ps, nl, cfg, ps->C_SL, MPS_WALL);
+}
+
 void oracle_viscosity(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg)
 {
     double re = cfg->influence_radius_lap;
@@ -1163,7 +1245,7 @@ int oracle_step_driven(ParticleSystem *ps, NeighborList *nl, CellList *cl, const
                        const double *rest, double amp, double freq, int axis, int step)
 {
     double re = fmax(cfg->influence_radius_lap, cfg->influence_radius_n);
-    if (cfg->surface_tension_enabled) return -2;   /* outside the restated path */
+    if (cfg->surface_tension_enabled) re = fmax(re, cfg->influence_radius_st);
     double dt = cfg->dt;
     int n = ps->num;
 
@@ -1172,6 +1254,10 @@ int oracle_step_driven(ParticleSystem *ps, NeighborList *nl, CellList *cl, const
         for (int d = 0; d < D; d++) p->acc[d] = (p->type == MPS_FLUID) ? cfg->gravity[d] : 0.0;
     }
     oracle_viscosity(ps, nl, cfg);
+    if (cfg->surface_tension_enabled) {
+        oracle_surface_tension(ps, nl, cfg);
+        oracle_surface_tension_SL(ps, nl, cfg);
+    }
     for (int i = 0; i < n; i++) {
         Particle *p = &ps->particles[i];
         if (p->type != MPS_FLUID) continue;

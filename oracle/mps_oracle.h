@@ -39,6 +39,8 @@ int  oracle_neighbor_search(NeighborList *nl, const ParticleSystem *ps,
 
 void oracle_number_density(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg);
 void oracle_viscosity(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg);
+void oracle_surface_tension(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg);
+void oracle_surface_tension_SL(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg);
 int  oracle_pressure_gradient(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg);
 void oracle_judge_free_surface(ParticleSystem *ps, double threshold);
 void oracle_neighbor_count(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg);

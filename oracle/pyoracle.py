@@ -57,6 +57,8 @@ class Oracle:
             "oracle_neighbor_search": (C.c_int, [NL, PS, CL, C.c_double]),
             "oracle_number_density": (None, [PS, NL, CF]),
             "oracle_viscosity": (None, [PS, NL, CF]),
+            "oracle_surface_tension": (None, [PS, NL, CF]),
+            "oracle_surface_tension_SL": (None, [PS, NL, CF]),
             "oracle_pressure_gradient": (C.c_int, [PS, NL, CF]),
             "oracle_judge_free_surface": (None, [PS, C.c_double]),
             "oracle_neighbor_count": (None, [PS, NL, CF]),

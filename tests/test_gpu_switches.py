@@ -11,7 +11,10 @@ same step from the same state and list, through the C ABI:
   * surface_detection_method 1: the neighbour-count surface test
     (operators.c:226-267), with its N0 from the initial parameters;
   * hs_mode 1 with the negative-pressure clamp (pressure_solver.c:342-362,
-    operators.c:188-199).
+    operators.c:188-199);
+  * surface tension with wetting (operators.c:281-354, 2-D operators.c:
+    231-309; coefficients of particle.c:185-211): the list radius grows to
+    influence_radius_st, the explicit stage adds the potential forces.
 
 Bit-exact: neighbour lists, number densities, neighbour counts, surface
 flags, types, the PPE matrix and right-hand side; pressures within 1e-8
@@ -37,6 +40,7 @@ SWITCHES = {
     "cmps1": dict(cmps_gradient=1),
     "cmps2_countsurf": dict(cmps_gradient=2, surface_detection_method=1),
     "hs1_clamp": dict(hs_mode=1, clamp_negative_pressure=1),
+    "surface_tension": dict(surface_tension_enabled=1, wetting_angle_SL=60.0),
 }
 
 
@@ -164,3 +168,32 @@ def test_cmps_gradient_stage_bitexact(cmps, dim):
     assert np.any(o["acc"] != hg.view["acc"])
     for f in ("acc", "vel", "pos", "pressure"):
         assert np.array_equal(g[f], o[f]), f
+
+
+@pytest.mark.parametrize("dim", [3, 2])
+def test_surface_tension_stages_bitexact(dim):
+    """calc_surface_tension and calc_surface_tension_SL alone, on the same
+    state and list, with the coefficients of the caller's particle system:
+    accelerations bit for bit."""
+    _cuda()
+    from mps_b200.session import Session
+    from oracle.pyoracle import Oracle
+    orc = Oracle(dim)
+    wl = _workload(dim, SWITCHES["surface_tension"])
+    cfg, hp, nl, cl = _moved(wl, orc)
+    assert hp.ps.C_LL > 0.0 and hp.ps.C_SL > 0.0
+    m = cfg.max_neighbors
+    L = orc.lib
+    for stage, fn, coeff in (("surface_tension", L.oracle_surface_tension, hp.ps.C_LL),
+                             ("surface_tension_sl", L.oracle_surface_tension_SL, hp.ps.C_SL)):
+        ho = hp.copy()
+        ho.view["acc"][:] = 0.0
+        hg = ho.copy()
+        fn(C.byref(ho.ps), C.byref(nl.nl), C.byref(cfg))
+        with Session(cfg, dim, hg.n) as s:
+            s.upload(hg)
+            s.set_initial_params(hp.ps.n0, hp.ps.lambda_, hp.ps.n0_count)
+            s.run_stage(stage, nl.neighbors[: hp.n * m], nl.count[: hp.n], m, arg=coeff)
+            g = s.download()
+        assert np.any(ho.view["acc"] != 0.0), stage
+        assert np.array_equal(g["acc"], ho.view["acc"]), stage

@@ -152,3 +152,41 @@ def test_oracle_reproduces_shipped_trajectory(oracle3):
     # contraction); they agree to the 8th significant digit.
     rel = np.abs(mine[:, 6] - g[:, 6]) / np.maximum(np.abs(g[:, 6]), 1.0)
     assert rel.max() < 1e-7
+
+
+@pytest.mark.parametrize("dim,kind,theta", [(3, "3d", 90.0), (3, "3d", 60.0), (2, "2d", 60.0)])
+def test_oracle_bitexact_surface_tension(dim, kind, theta, oracle3, oracle2):
+    """Surface tension (3P operators.c:281-354, 2D operators.c:231-309) with
+    its calibrated coefficients (particle.c:185-211): C_LL and C_SL equal the
+    reference's, and so does every field after several steps; the C ABI's
+    mps_surface_tension_coeffs gives the same coefficients."""
+    from mps_b200 import _lib
+    ref = reference_lib(kind)
+    orc = oracle3 if dim == 3 else oracle2
+    sw = dict(surface_tension_enabled=1, surface_tension_coeff=0.0728, surface_tension_re_ratio=3.2,
+              wetting_angle_SL=theta)
+    wl = (W.small_dambreak3d(l0=0.025, seed=7, **sw) if dim == 3 else W.small_dambreak2d(l0=0.02, seed=7, **sw))
+    cfg = wl.config()
+    assert cfg.surface_tension_enabled == 1 and cfg.influence_radius_st > cfg.influence_radius_lap
+    hp_o, nl_o, cl_o = _setup(orc, wl, cfg)
+    hp_r = T.HostParticles(dim, wl.pos, wl.vel, wl.types)
+    ref.set_config(cfg)
+    ref.lib.particle_system_calc_initial_params(C.byref(hp_r.ps))
+    assert hp_o.ps.C_LL == hp_r.ps.C_LL and hp_o.ps.C_LL > 0.0
+    assert hp_o.ps.C_SL == hp_r.ps.C_SL
+    lib = _lib.load()
+    cll, csl = C.c_double(), C.c_double()
+    p = _lib.params_from_config(cfg, dim)
+    assert lib.mps_surface_tension_coeffs(C.byref(p), C.byref(cll), C.byref(csl)) == 0
+    assert (cll.value, csl.value) == (hp_r.ps.C_LL, hp_r.ps.C_SL)
+    re = CF.neighbor_radius(cfg)
+    nl_r = T.HostNeighborList(hp_r.n, cfg.max_neighbors)
+    cl_r = ref.cell_list(hp_r.n, re, cfg)
+    ref.lib.neighbor_search_cell_linked_list(C.byref(nl_r.nl), C.byref(hp_r.ps), cl_r, re)
+    for s in range(1, 4):
+        assert orc.step(hp_o, nl_o, cl_o, cfg) == 0
+        ref.step(hp_r, nl_r, cl_r, s)
+        for f in FIELDS:
+            assert np.array_equal(hp_o.view[f], hp_r.view[f]), (s, f)
+        assert np.array_equal(nl_o.count, nl_r.count)
+    ref.lib.cell_list_free(cl_r)
