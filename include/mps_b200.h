@@ -349,8 +349,13 @@ int  mps_adjoint_get(mps_session *s, double *lam_pos, double *lam_vel, double *g
  * Limits: num <= MPS_NOALLOC_MAX_PARTICLES, total cells <=
  * MPS_NOALLOC_MAX_CELLS; larger requests return MPS_ERR_INVALID.  The first
  * call on a device looks up the static array's device address and should
- * come before any stream capture.  All calls share that array: calls whose
- * work overlaps on the GPU race on it and must be ordered by the caller. */
+ * come before any stream capture.  The address is kept for the life of the
+ * process; a cudaDeviceReset (or any reset of the device's primary context)
+ * unloads the library's module and makes it stale, so no call may follow
+ * one.  All calls share that array: calls whose work overlaps on the GPU
+ * race on it and must be ordered by the caller.  A CUDA error already
+ * pending in the calling thread is returned as MPS_ERR_CUDA without being
+ * cleared, and no work is queued. */
 #define MPS_NOALLOC_MAX_PARTICLES 262144
 #define MPS_NOALLOC_MAX_CELLS     262144
 

@@ -147,6 +147,9 @@ extern "C" int mps_cell_sort_noalloc(const mps_grid_t *grid, const double *pos, 
         return MPS_ERR_INVALID;
     }
     if (!(grid->cell_size > 0.0)) return MPS_ERR_INVALID;
+    // an error already pending in the caller's context is theirs: report it
+    // without clearing it, and queue no work
+    if (cudaPeekAtLastError() != cudaSuccess) return MPS_ERR_CUDA;
     int *scratch = nullptr;
     int rc = scratch_for_current_device(&scratch);
     if (rc != MPS_OK) return rc;
@@ -176,5 +179,6 @@ extern "C" int mps_cell_sort_noalloc(const mps_grid_t *grid, const double *pos, 
         mps::launch(k_na_rank, nb, B, 0, st, (const int *)cell_start + tot, (const int *)slot, (const int *)cell,
                     (const int *)cell_start, order);
     }
-    return cudaGetLastError() == cudaSuccess ? MPS_OK : MPS_ERR_CUDA;
+    // a failed launch of this call stays pending for the caller to see
+    return cudaPeekAtLastError() == cudaSuccess ? MPS_OK : MPS_ERR_CUDA;
 }

@@ -98,6 +98,24 @@ def test_cell_sort_noalloc_matches_session_twice():
         _check(cell, order, start, exp_cell, head, nxt, total, wl.n)
 
 
+def test_cell_sort_noalloc_matches_session_twice_2d():
+    """The 2-D grid (cell = iy * nx + ix, positions two per particle)."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from mps_b200 import _lib
+    lib = _lib.load()
+    runs = [W.small_dambreak2d(l0=0.01, seed=33), W.small_dambreak2d(l0=0.01, seed=34)]
+    runs[0].types[7] = T.GHOST
+    for wl in runs:
+        cfg = wl.config()
+        exp_cell, head, nxt, total = _expected(cfg, 2, wl)
+        g = _grid(cfg, 2)
+        rc, cell, order, start = _call(lib, g, wl, 2, torch)
+        assert rc == 0
+        _check(cell, order, start, exp_cell, head, nxt, total, wl.n)
+
+
 def test_cell_sort_noalloc_rejects_oversize():
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
