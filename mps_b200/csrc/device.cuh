@@ -81,7 +81,6 @@ enum : unsigned {
     ERR_COLORING          = 8u,   // matrix couples two same-coloured cells
     ERR_CELL_OVERFULL     = 16u,  // more than 255 unknowns in one cell
     ERR_COPY_TIMEOUT      = 32u,  // a bulk copy into shared memory did not complete in time
-    ERR_WINDOW_OVERFLOW   = 64u,  // a window of block inverses exceeded its shared-memory stage
     ERR_GRID_TIMEOUT      = 128u, // a grid barrier of the persistent PCG kernel did not complete in time
 };
 

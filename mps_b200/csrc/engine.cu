@@ -301,6 +301,8 @@ private:
     // entries per lane loaded in one batch by k_sweep_colour's head sums
     // (MPS_SWEEP_HB: 4 or 8)
     int head_batch_ = 4;
+    // CTAs per SM the colour sweep is compiled for (MPS_SWEEP_OCC: 6 or 8)
+    int sweep_occ_ = 6;
     // polls of the first wait for a staged block inverse (MPS_TEST_MBAR_POLLS
     // lowers it, down to 0, to exercise the timeout path)
     int first_polls_ = MBAR_POLLS;
@@ -457,6 +459,7 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
         sweep_mode_ = (v == 0 || v == 1) ? v : 2;
     }
     if (const char *e = std::getenv("MPS_SWEEP_HB")) head_batch_ = std::atoi(e) == 8 ? 8 : 4;
+    if (const char *e = std::getenv("MPS_SWEEP_OCC")) sweep_occ_ = std::atoi(e) == 8 ? 8 : 6;
     if (const char *e = std::getenv("MPS_PCG_BATCH")) {
         int v = std::atoi(e);
         if (v >= 1 && v <= 1024) pcg_batch_ = v;
@@ -747,7 +750,6 @@ void Engine<D>::check_err()
         if (e & ERR_CELL_OVERFULL) throw CudaError("more than 255 PPE unknowns in one cell", MPS_ERR_UNSUPPORTED);
         if (e & ERR_COPY_TIMEOUT) throw CudaError("a bulk copy into shared memory timed out", MPS_ERR_CUDA);
         if (e & ERR_GRID_TIMEOUT) throw CudaError("a grid barrier of the persistent PCG kernel timed out", MPS_ERR_CUDA);
-        if (e & ERR_WINDOW_OVERFLOW) throw CudaError("in-cell inverse window exceeds its stage", MPS_ERR_INVALID);
         throw CudaError("device error", MPS_ERR_INVALID);
     }
 }
@@ -1359,16 +1361,23 @@ void Engine<D>::run_sweep(const PcgBufs<TM> &v, bool fwdir)
         }
         auto colk = fwdir ? k_sweep_colour<true, TM> : k_sweep_colour<false, TM>;
         if (head_batch_ == 8) colk = fwdir ? k_sweep_colour<true, TM, 8> : k_sweep_colour<false, TM, 8>;
+        // 8 CTAs per SM: 32 registers per thread and, in FP64, a stage that
+        // holds the window plus one cell of up to 40 unknowns
+        int stage = win_ + CELL_MAXBLK;
+        if (sweep_occ_ == 8) {
+            colk = fwdir ? k_sweep_colour<true, TM, 4, 8> : k_sweep_colour<false, TM, 4, 8>;
+            if (sizeof(TM) == 8) stage = win_ + 824;
+        }
         for (int i = 0; i < nc; i++) {
             int c = order[i], cn = i + 1 < nc ? order[i + 1] : -1;
             int nrb = cn >= 0 ? row_off_[cn] : 0, nre = cn >= 0 ? row_off_[cn + 1] : 0;
             int ncb = cn >= 0 ? nblk((long long)(nre - nrb) * 8, CELL_THREADS) : 0;
-            lk(2, colk, nwin_[c] + ncb, CELL_THREADS, sizeof(TM) * (win_ + CELL_MAXBLK),
+            lk(2, colk, nwin_[c] + ncb, CELL_THREADS, sizeof(TM) * stage,
                (const int *)wfirst_.p + win_off_[c], nwin_[c], (const int2 *)adesc_.p, (const int *)inv_off_.p,
                fwdir ? v.inv_cm : v.inv_rm, pko, pkl, pkv, pkk, v.dinv, (const int *)(fwdir ? xp_lo_.p : xp_up_.p),
                (const int *)(fwdir ? xs_lo_.p : xs_up_.p), (const int *)(fwdir ? xc_lo_.p : xc_up_.p),
                fwdir ? v.xf_lo : v.xf_up, (int)(i == 0), nrb, nre, rhs, v.part, out, (const CGScalars *)sc_.p,
-               win_ + CELL_MAXBLK, first_polls_, err_.p);
+               stage, first_polls_, err_.p);
         }
     }
 }

@@ -748,8 +748,8 @@ __global__ void k_gather_colour_offsets(ColourIdx at, int n, const int *__restri
 // dependent: what it loads before pdl_wait() (row bounds, factor values and
 // columns, block inverses, cell descriptors) is written once per step,
 // before the CG loop; x, part and the CG scalars are read only after it.
-template <bool FWD, class TM, int HB = 4>
-__global__ void __launch_bounds__(CELL_THREADS, 6)
+template <bool FWD, class TM, int HB = 4, int MINB = 6>
+__global__ void __launch_bounds__(CELL_THREADS, MINB)
 k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict__ desc,
                const int *__restrict__ inv_off, const TM *__restrict__ inv, const int *__restrict__ pk_off,
                const int *__restrict__ pk_len, const TM *__restrict__ pk_val, const unsigned char *__restrict__ pk_k,
@@ -850,7 +850,7 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
     __syncthreads();
     // on a timeout the copy is still waited for (long bound) before the CTA returns
     if (staged && !stage_wait(b, first_polls, err)) return;
-    if (nel > stage_elems && threadIdx.x == 0) atomicOr(err, ERR_WINDOW_OVERFLOW);
+    // a window larger than the stage reads its block inverses from global memory
     if (done) return;
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const TM *src = staged ? stage : inv + o0;
