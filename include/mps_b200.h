@@ -97,6 +97,14 @@ typedef struct {
     double influence_radius_st;
     double surface_tension_coeff;
     double wetting_angle_SL;
+    /* Hybrid contact-line friction of the 3-D serial variant
+     * (mps_fluid3D/src/operators.c:337-492; 3-D only): static below the
+     * velocity threshold (m/s) within delta_theta (degrees) of the contact
+     * angle wetting_angle_SL, dynamic damping with alpha above it. */
+    int    friction_enabled;
+    double friction_delta_theta;
+    double dynamic_friction_alpha;
+    double friction_velocity_threshold;
 } mps_params_t;
 
 /* Per-step metrics (the reference computes and discards its iteration count,

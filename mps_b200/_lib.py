@@ -79,6 +79,10 @@ class MpsParams(C.Structure):
         ("influence_radius_st", C.c_double),
         ("surface_tension_coeff", C.c_double),
         ("wetting_angle_SL", C.c_double),
+        ("friction_enabled", C.c_int),
+        ("friction_delta_theta", C.c_double),
+        ("dynamic_friction_alpha", C.c_double),
+        ("friction_velocity_threshold", C.c_double),
     ]
 
 
@@ -219,6 +223,9 @@ def params_from_config(cfg, dim: int, precision: int = PREC_FP64, refine_toleran
         p.gravity[d] = cfg.gravity[d]
         p.domain_min[d] = cfg.domain_min[d]
         p.domain_max[d] = cfg.domain_max[d]
+    from .types import FRICTION_DEFAULTS
+    for f, v in FRICTION_DEFAULTS.items():   # 3-D serial-variant keys, config attributes when parsed
+        setattr(p, f, getattr(cfg, f, v))
     p.precision = precision
     p.refine_tolerance = refine_tolerance
     return p

@@ -174,6 +174,12 @@ def _param_table(dim: int):
         "hs_mode": ("hs_mode", i),
     }
     if dim == 3:
+        # the 3-D serial variant's friction keys (mps_fluid3D/src/sim_config.c:267-274),
+        # kept as attributes of the config: the OpenMP layout has no such fields
+        t["friction_enabled"] = ("friction_enabled", i)
+        t["friction_delta_theta"] = ("friction_delta_theta", f)
+        t["dynamic_friction_alpha"] = ("dynamic_friction_alpha", f)
+        t["friction_velocity_threshold"] = ("friction_velocity_threshold", f)
         t["gravity_z"] = (("gravity", 2), f)
         t["domain_z_min"] = (("domain_min", 2), f)
         t["domain_z_max"] = (("domain_max", 2), f)

@@ -120,6 +120,9 @@ struct Consts {
     int    st_on, st_sl_on;        // surface tension; its wall term (C_SL != 0)
     double st_ll, st_sl;           // C_LL / (rho l0^D), C_SL / (rho l0^D)   operators.c:284, :326
     double re_st, st_rmin;         // influence_radius_st, 1e-9 * l0          operators.c:303
+    int    fr_on;                  // contact-line friction (3-D serial variant operators.c:337)
+    double fr_theta_s, fr_dtheta;  // wetting angle, critical deviation (radians)   :341-342
+    double fr_vc, fr_dyn;          // velocity threshold; alpha nu 2D / (n0 lambda)  :343-346
 };
 
 // Structure-of-arrays particle state.  `key` holds the positions at the

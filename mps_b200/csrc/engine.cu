@@ -443,6 +443,7 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
     if (p.dim != D) throw CudaError("dimension mismatch", MPS_ERR_INVALID);
     if (capacity <= 0) throw CudaError("capacity must be positive", MPS_ERR_INVALID);
     if (p.wall_drive_axis < 0 || p.wall_drive_axis >= D) throw CudaError("wall_drive_axis out of range", MPS_ERR_INVALID);
+    if (D == 2 && p.friction_enabled) throw CudaError("friction is a 3-D model", MPS_ERR_UNSUPPORTED);
     cap_ = capacity;
     prm_ = p;
     if (const char *e = std::getenv("MPS_SPMV_LPR")) {
@@ -707,6 +708,12 @@ void Engine<D>::compute_consts()
     k.st_sl_on = csl != 0.0;
     k.re_st = p.influence_radius_st;
     k.st_rmin = 1.0e-9 * l0;
+    // friction (3S operators.c:341-346), with the reference's expressions
+    k.fr_on = D == 3 && p.friction_enabled != 0;
+    k.fr_theta_s = p.wetting_angle_SL * M_PI / 180.0;
+    k.fr_dtheta = p.friction_delta_theta * M_PI / 180.0;
+    k.fr_vc = p.friction_velocity_threshold;
+    k.fr_dyn = p.dynamic_friction_alpha * p.viscosity * 2.0 * D / (n0 * lambda);
 }
 
 template <int D>
@@ -714,6 +721,7 @@ void Engine<D>::update_params(const mps_params_t &p)
 {
     if (p.dim != D) throw CudaError("dimension mismatch", MPS_ERR_INVALID);
     if (p.wall_drive_axis < 0 || p.wall_drive_axis >= D) throw CudaError("wall_drive_axis out of range", MPS_ERR_INVALID);
+    if (D == 2 && p.friction_enabled) throw CudaError("friction is a 3-D model", MPS_ERR_UNSUPPORTED);
     bool regrid = false;
     for (int d = 0; d < D; d++)
         regrid |= p.domain_min[d] != prm_.domain_min[d] || p.domain_max[d] != prm_.domain_max[d];
@@ -1028,7 +1036,14 @@ void Engine<D>::explicit_stage(bool from_list)
         if (from_list) launch(k_surface_tension<D, ListSource>, nb, TPB, 0, st_, list(), S(), k_, n, 3);
         else launch(k_surface_tension<D, CellSource<D>>, nb, TPB, 0, st_, cells(), S(), k_, n, 3);
     }
-    launch(k_explicit_update<D>, nb, TPB, 0, st_, S(), k_, n);
+    if (k_.fr_on) {
+        launch(k_explicit_part<D>, nb, TPB, 0, st_, S(), k_, n, 1);
+        if (from_list) launch(k_friction<D, ListSource>, nb, TPB, 0, st_, list(), S(), k_, n);
+        else launch(k_friction<D, CellSource<D>>, nb, TPB, 0, st_, cells(), S(), k_, n);
+        launch(k_explicit_part<D>, nb, TPB, 0, st_, S(), k_, n, 2);
+    } else {
+        launch(k_explicit_update<D>, nb, TPB, 0, st_, S(), k_, n);
+    }
     if (k_.drive_on) {
         double dx, vel;
         drive_terms((double)(tstep_ + 1) * prm_.dt, &dx, &vel);
@@ -1965,8 +1980,9 @@ void Engine<D>::step_adjoint()
     require_ref();
     if (!structure_) throw CudaError("no neighbour structure: load a checkpoint first", MPS_ERR_INVALID);
     if (prm_.hs_mode != 0 || prm_.ppe_type != 0 || prm_.cmps_gradient != 0 || prm_.clamp_negative_pressure ||
-        prm_.surface_tension_enabled)
-        throw CudaError("the adjoint supports hs_mode 0, ppe_type 0, cmps_gradient 0, no clamp",
+        prm_.surface_tension_enabled || prm_.friction_enabled)
+        throw CudaError("the adjoint supports hs_mode 0, ppe_type 0, cmps_gradient 0, no clamp, no surface tension "
+                        "or friction",
                         MPS_ERR_UNSUPPORTED);
     ensure_adj();
     bool pseed = pseed_on_;   // consumed by this call

@@ -89,6 +89,149 @@ __global__ void k_surface_tension(Src src, State<D> s, Consts k, int n, int whic
     for (int d = 0; d < D; d++) s.acc[d][i] = a[d];
 }
 
+// Hybrid contact-line friction of the 3-D serial variant (mps_fluid3D
+// operators.c:337-492), between the velocity and the position updates.  A
+// fluid particle with a wall neighbour within re_st (the nearest, first in
+// list order, is j*) and a fluid-only number density below the surface
+// threshold is on the contact line.  Its wall normal comes from the walls in
+// j*'s list, its free-surface normal from its fluid neighbours (weights
+// w(r, re_st)), cos theta = -n_w . n_lv, and the slide direction is n_lv
+// projected on the wall's tangent plane.  Slow particles (|v| <= v_c) stop
+// when theta is within dtheta of the wetting angle; fast ones lose a share of
+// their slide velocity, clipped so it never reverses.  Each thread changes
+// only its own velocity, from positions that no thread changes here.
+template <int D, class Src>
+__global__ void k_friction(Src src, State<D> s, Consts k, int n)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || s.type[i] != FLUID) return;
+    double pi[D];
+    load_vec<D>(pi, s.pos, i);
+    double re_st2 = k.re_st * k.re_st, re_n2 = k.re_n * k.re_n;
+    double n_fluid = 0.0, r2_star = 1.0e30;
+    int j_star = -1;
+    src.for_each(i, [&](int j) {
+        double pj[D];
+        load_vec<D>(pj, s.pos, j);
+        double r2 = dist2<D>(pi, pj);
+        if (s.type[j] == FLUID) {
+            if (r2 < re_n2) n_fluid += kweight(sqrt(r2), k.re_n, k.rmin);
+        } else if (s.type[j] == WALL) {
+            if (r2 < re_st2 && r2 < r2_star) {
+                r2_star = r2;
+                j_star = j;
+            }
+        }
+    });
+    if (j_star < 0 || n_fluid >= k.surf_thr) return;
+    double ps[D], nw[D], nlv[D];
+    load_vec<D>(ps, s.pos, j_star);
+#pragma unroll
+    for (int d = 0; d < D; d++) nw[d] = nlv[d] = 0.0;
+    src.for_each(j_star, [&](int m) {
+        if (s.type[m] != WALL) return;
+        double pm[D], dr[D], r2 = 0.0;
+        load_vec<D>(pm, s.pos, m);
+#pragma unroll
+        for (int d = 0; d < D; d++) {
+            dr[d] = ps[d] - pm[d];
+            r2 += dr[d] * dr[d];
+        }
+        double r = sqrt(r2);
+        if (r < k.st_rmin) return;
+        double w = kweight(r, k.re_st, k.rmin);
+#pragma unroll
+        for (int d = 0; d < D; d++) nw[d] += w * dr[d] / r;
+    });
+    double mag = 0.0;
+#pragma unroll
+    for (int d = 0; d < D; d++) mag += nw[d] * nw[d];
+    mag = sqrt(mag);
+    if (mag < 1.0e-9) return;
+#pragma unroll
+    for (int d = 0; d < D; d++) nw[d] /= mag;
+    int fluid_count = 0;
+    src.for_each(i, [&](int j) {
+        if (s.type[j] != FLUID) return;
+        double pj[D], dr[D];
+        load_vec<D>(pj, s.pos, j);
+        double r = sqrt(dist2v<D>(pi, pj, dr));
+        if (r < k.st_rmin) return;
+        double w = kweight(r, k.re_st, k.rmin);
+#pragma unroll
+        for (int d = 0; d < D; d++) nlv[d] -= w * dr[d] / r;
+        fluid_count++;
+    });
+    if (fluid_count == 0) return;
+    mag = 0.0;
+#pragma unroll
+    for (int d = 0; d < D; d++) mag += nlv[d] * nlv[d];
+    mag = sqrt(mag);
+    if (mag < 1.0e-9) return;
+#pragma unroll
+    for (int d = 0; d < D; d++) nlv[d] /= mag;
+    double cos_th = 0.0;
+#pragma unroll
+    for (int d = 0; d < D; d++) cos_th -= nw[d] * nlv[d];
+    cos_th = fmax(-1.0, fmin(1.0, cos_th));
+    double theta = acos(cos_th);
+    double dot = 0.0;
+#pragma unroll
+    for (int d = 0; d < D; d++) dot += nlv[d] * nw[d];
+    double e[D], emag = 0.0;
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+        e[d] = nlv[d] - dot * nw[d];
+        emag += e[d] * e[d];
+    }
+    emag = sqrt(emag);
+    if (emag < 1.0e-9) return;
+#pragma unroll
+    for (int d = 0; d < D; d++) e[d] /= emag;
+    double v[D], v2 = 0.0;
+    load_vec<D>(v, s.vel, i);
+#pragma unroll
+    for (int d = 0; d < D; d++) v2 += v[d] * v[d];
+    if (sqrt(v2) <= k.fr_vc) {
+        if (fabs(theta - k.fr_theta_s) <= k.fr_dtheta) {
+#pragma unroll
+            for (int d = 0; d < D; d++) s.vel[d][i] = 0.0;
+        }
+        return;
+    }
+    double sum_w = 0.0;
+    src.for_each(i, [&](int j) {
+        if (s.type[j] != WALL) return;
+        double pj[D];
+        load_vec<D>(pj, s.pos, j);
+        double r = sqrt(dist2<D>(pi, pj));
+        if (r < k.st_rmin) return;
+        sum_w += kweight(r, k.re_st, k.rmin);
+    });
+    double vn = 0.0;
+#pragma unroll
+    for (int d = 0; d < D; d++) vn += v[d] * e[d];
+    double dvn = -k.fr_dyn * k.dt * sum_w * vn;
+    if (dvn > vn) dvn = vn;
+    if (dvn < -vn) dvn = -vn;
+#pragma unroll
+    for (int d = 0; d < D; d++) s.vel[d][i] = v[d] + dvn * e[d];
+}
+
+// The explicit update in two passes, friction between them (3S
+// simulation.c:43-60): mode 1, u* = u + dt a; mode 2, r* = r + dt u*.
+template <int D>
+__global__ void k_explicit_part(State<D> s, Consts k, int n, int mode)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || s.type[i] != FLUID) return;
+#pragma unroll
+    for (int d = 0; d < D; d++) {
+        if (mode == 1) s.vel[d][i] = s.vel[d][i] + k.dt * s.acc[d][i];
+        else s.pos[d][i] = s.pos[d][i] + k.dt * s.vel[d][i];
+    }
+}
+
 template <int D>
 __global__ void k_explicit_update(State<D> s, Consts k, int n)
 {

@@ -117,10 +117,38 @@ def _sim_config_type(dim: int):
     return type(f"SimConfig{dim}", (C.Structure,), {"_fields_": fields})
 
 
+def _serial_config_type():
+    """SimConfig of the 3-D serial variant (mps_fluid3D/include/sim_config.h):
+    the OpenMP layout with four friction fields after hs_mode."""
+    fields = []
+    for name, t in _sim_config_type(3)._fields_:
+        fields.append((name, t))
+        if name == "hs_mode":
+            fields += [("friction_enabled", C.c_int), ("friction_delta_theta", C.c_double),
+                       ("dynamic_friction_alpha", C.c_double), ("friction_velocity_threshold", C.c_double)]
+    return type("SimConfig3S", (C.Structure,), {"_fields_": fields})
+
+
+FRICTION_DEFAULTS = {"friction_enabled": 0, "friction_delta_theta": 30.0, "dynamic_friction_alpha": 600.0,
+                     "friction_velocity_threshold": 0.01}   # mps_fluid3D/src/sim_config.c:76-79
+
+
+def serial_config(cfg):
+    """A SimConfig3S copy of a 3-D config; the friction fields come from the
+    config's attributes of the same names, else the serial variant's defaults."""
+    out = SimConfig3S()
+    for name, _ in SimConfig3._fields_:
+        setattr(out, name, getattr(cfg, name))
+    for name, v in FRICTION_DEFAULTS.items():
+        setattr(out, name, getattr(cfg, name, v))
+    return out
+
+
 CellList3 = _cell_list_type(3)
 CellList2 = _cell_list_type(2)
 SimConfig3 = _sim_config_type(3)
 SimConfig2 = _sim_config_type(2)
+SimConfig3S = _serial_config_type()
 
 
 def sim_config_type(dim: int):

@@ -467,6 +467,132 @@ void oracle_surface_tension_SL(ParticleSystem *ps, const NeighborList *nl, const
     surface_tension_pass(ps, nl, cfg, ps->C_SL, MPS_WALL);
 }
 
+/* Hybrid static / dynamic friction at the contact line, 3S (mps_fluid3D)
+ * operators.c:337-492.  The friction parameters live in the 3-D serial
+ * variant's SimConfig only, so they are set apart (oracle_set_friction).
+ * For every fluid particle i, with its list: the fluid-only number density
+ * n_f (re_n) and the nearest wall particle j* within re_st; a contact-line
+ * particle has j* and n_f < surface_threshold * n0.  The wall normal n_w is
+ * the normalised sum of w(r, re_st) (j* - k)/r over the walls k in j*'s
+ * list, the free-surface normal n_lv the normalised -sum of w(r, re_st)
+ * (j - i)/r over i's fluid neighbours, cos theta_i = -n_w . n_lv, and the
+ * slide direction e the normalised projection of n_lv on the wall's tangent
+ * plane.  Static (|v_i| <= v_c): v_i = 0 when |theta_i - theta_s| <= dtheta.
+ * Dynamic: v_n = v_i . e damped by dv_n = -alpha nu (2D / (n0 lambda)) dt
+ * (sum of w(r, re_st) over wall neighbours) v_n, clipped to |v_n|.  Each
+ * particle changes only its own velocity from positions and its own
+ * velocity, so the loop order does not matter. */
+#if D == 3
+static OracleFriction g_friction = {0, 30.0, 600.0, 0.01};
+
+void oracle_set_friction(const OracleFriction *f) { g_friction = *f; }
+
+void oracle_apply_friction(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg)
+{
+    if (!g_friction.enabled) return;
+    double re_st = cfg->influence_radius_st;
+    double l0 = cfg->particle_distance;
+    double theta_s = cfg->wetting_angle_SL * M_PI / 180.0;
+    double delta_th = g_friction.delta_theta * M_PI / 180.0;
+    double v_c = g_friction.velocity_threshold;
+    double alpha = g_friction.alpha;
+    double nu = cfg->viscosity;
+    double dyn_coeff = alpha * nu * 2.0 * D / (ps->n0 * ps->lambda);
+    double re_n = cfg->influence_radius_n;
+    double surf_thr = cfg->surface_threshold;
+    for (int i = 0; i < ps->num; i++) {
+        Particle *pi = &ps->particles[i];
+        if (pi->type != MPS_FLUID) continue;
+        double n_fluid = 0.0, r2_star = 1.0e30;
+        int j_star = -1;
+        for (int k = 0; k < nl->count[i]; k++) {
+            int j = NB(nl, i, k);
+            double r2 = dist2(pi->pos, ps->particles[j].pos);
+            if (ps->particles[j].type == MPS_FLUID) {
+                if (r2 < re_n * re_n) n_fluid += KW(sqrt(r2), re_n);
+            } else if (ps->particles[j].type == MPS_WALL) {
+                if (r2 < re_st * re_st && r2 < r2_star) { r2_star = r2; j_star = j; }
+            }
+        }
+        if (j_star < 0) continue;
+        if (n_fluid >= surf_thr * ps->n0) continue;
+        const Particle *ps_ = &ps->particles[j_star];
+        double n_w[D] = {0.0, 0.0, 0.0};
+        for (int k = 0; k < nl->count[j_star]; k++) {
+            int m = NB(nl, j_star, k);
+            if (ps->particles[m].type != MPS_WALL) continue;
+            double dr[D], r2 = 0.0;
+            for (int d = 0; d < D; d++) {
+                dr[d] = ps_->pos[d] - ps->particles[m].pos[d];
+                r2 += dr[d] * dr[d];
+            }
+            double r = sqrt(r2);
+            if (r < 1.0e-9 * l0) continue;
+            double w = KW(r, re_st);
+            for (int d = 0; d < D; d++) n_w[d] += w * dr[d] / r;
+        }
+        double n_w_mag = 0.0;
+        for (int d = 0; d < D; d++) n_w_mag += n_w[d] * n_w[d];
+        n_w_mag = sqrt(n_w_mag);
+        if (n_w_mag < 1.0e-9) continue;
+        for (int d = 0; d < D; d++) n_w[d] /= n_w_mag;
+        double n_lv[D] = {0.0, 0.0, 0.0};
+        int fluid_count = 0;
+        for (int k = 0; k < nl->count[i]; k++) {
+            int j = NB(nl, i, k);
+            if (ps->particles[j].type != MPS_FLUID) continue;
+            double dr[D];
+            double r = sqrt(dist2_vec(pi->pos, ps->particles[j].pos, dr));
+            if (r < 1.0e-9 * l0) continue;
+            double w = KW(r, re_st);
+            for (int d = 0; d < D; d++) n_lv[d] -= w * dr[d] / r;
+            fluid_count++;
+        }
+        if (fluid_count == 0) continue;
+        double n_lv_mag = 0.0;
+        for (int d = 0; d < D; d++) n_lv_mag += n_lv[d] * n_lv[d];
+        n_lv_mag = sqrt(n_lv_mag);
+        if (n_lv_mag < 1.0e-9) continue;
+        for (int d = 0; d < D; d++) n_lv[d] /= n_lv_mag;
+        double cos_th = 0.0;
+        for (int d = 0; d < D; d++) cos_th -= n_w[d] * n_lv[d];
+        cos_th = fmax(-1.0, fmin(1.0, cos_th));
+        double theta_i = acos(cos_th);
+        double dot_lv_w = 0.0;
+        for (int d = 0; d < D; d++) dot_lv_w += n_lv[d] * n_w[d];
+        double e_slide[D], e_slide_mag = 0.0;
+        for (int d = 0; d < D; d++) {
+            e_slide[d] = n_lv[d] - dot_lv_w * n_w[d];
+            e_slide_mag += e_slide[d] * e_slide[d];
+        }
+        e_slide_mag = sqrt(e_slide_mag);
+        if (e_slide_mag < 1.0e-9) continue;
+        for (int d = 0; d < D; d++) e_slide[d] /= e_slide_mag;
+        double v2 = 0.0;
+        for (int d = 0; d < D; d++) v2 += pi->vel[d] * pi->vel[d];
+        if (sqrt(v2) <= v_c) {
+            if (fabs(theta_i - theta_s) <= delta_th)
+                for (int d = 0; d < D; d++) pi->vel[d] = 0.0;
+        } else {
+            double sum_w_wall = 0.0;
+            for (int k = 0; k < nl->count[i]; k++) {
+                int j = NB(nl, i, k);
+                if (ps->particles[j].type != MPS_WALL) continue;
+                double r = sqrt(dist2(pi->pos, ps->particles[j].pos));
+                if (r < 1.0e-9 * l0) continue;
+                sum_w_wall += KW(r, re_st);
+            }
+            double v_n = 0.0;
+            for (int d = 0; d < D; d++) v_n += pi->vel[d] * e_slide[d];
+            double dv_n = -dyn_coeff * cfg->dt * sum_w_wall * v_n;
+            if (dv_n > v_n) dv_n = v_n;
+            if (dv_n < -v_n) dv_n = -v_n;
+            for (int d = 0; d < D; d++) pi->vel[d] += dv_n * e_slide[d];
+        }
+    }
+}
+#endif
+
 void oracle_viscosity(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg)
 {
     double re = cfg->influence_radius_lap;
@@ -1263,6 +1389,9 @@ int oracle_step_driven(ParticleSystem *ps, NeighborList *nl, CellList *cl, const
         if (p->type != MPS_FLUID) continue;
         for (int d = 0; d < D; d++) p->vel[d] += dt * p->acc[d];
     }
+#if D == 3
+    oracle_apply_friction(ps, nl, cfg);   /* 3S simulation.c:52-53 */
+#endif
     for (int i = 0; i < n; i++) {
         Particle *p = &ps->particles[i];
         if (p->type != MPS_FLUID) continue;

@@ -41,6 +41,16 @@ void oracle_number_density(ParticleSystem *ps, const NeighborList *nl, const Sim
 void oracle_viscosity(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg);
 void oracle_surface_tension(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg);
 void oracle_surface_tension_SL(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg);
+/* Friction of the 3-D serial variant (3-D builds only): its four SimConfig
+ * fields, kept apart because the OpenMP layout has none; off by default. */
+typedef struct {
+    int    enabled;
+    double delta_theta;          /* degrees */
+    double alpha;
+    double velocity_threshold;   /* m/s */
+} OracleFriction;
+void oracle_set_friction(const OracleFriction *f);
+void oracle_apply_friction(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg);
 int  oracle_pressure_gradient(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg);
 void oracle_judge_free_surface(ParticleSystem *ps, double threshold);
 void oracle_neighbor_count(ParticleSystem *ps, const NeighborList *nl, const SimConfig *cfg);

@@ -75,12 +75,26 @@ class Oracle:
             "oracle_cell_inverses": (None, [C.c_int, P, P, P, P, P, C.c_int, P]),
             "oracle_ic0_apply_csr": (None, [C.c_int, P, P, P, P, P]),
             "oracle_last_iterations": (C.c_int, []),
+            **({"oracle_set_friction": (None, [P]), "oracle_apply_friction": (None, [PS, NL, CF])} if dim == 3 else {}),
             "oracle_last_residual": (C.c_double, []),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
             f.restype = res
             f.argtypes = args
+
+    def set_friction(self, cfg) -> None:
+        """The friction parameters of the 3-D serial variant (3-D only), from
+        the config's attributes (mps_b200.types.FRICTION_DEFAULTS otherwise)."""
+        class _F(C.Structure):
+            _fields_ = [("enabled", C.c_int), ("delta_theta", C.c_double), ("alpha", C.c_double),
+                        ("velocity_threshold", C.c_double)]
+        d = T.FRICTION_DEFAULTS
+        f = _F(int(getattr(cfg, "friction_enabled", d["friction_enabled"])),
+               float(getattr(cfg, "friction_delta_theta", d["friction_delta_theta"])),
+               float(getattr(cfg, "dynamic_friction_alpha", d["dynamic_friction_alpha"])),
+               float(getattr(cfg, "friction_velocity_threshold", d["friction_velocity_threshold"])))
+        self.lib.oracle_set_friction(C.byref(f))
 
     # --- convenience wrappers -------------------------------------------------
     def ic0_csr(self, rp, ci, v):
@@ -164,7 +178,7 @@ class Reference:
     points it at a caller-owned struct, as the reference's main.c does.
     """
 
-    LIBS = {"3d": ("libref3d.so", 3), "2d": ("libref2d.so", 2)}
+    LIBS = {"3d": ("libref3d.so", 3), "2d": ("libref2d.so", 2), "3s": ("libref3s.so", 3)}
 
     def __init__(self, kind: str = "3d"):
         fname, dim = self.LIBS[kind]
@@ -205,6 +219,10 @@ class Reference:
         self._cfg_ref = None
 
     def set_config(self, cfg) -> None:
+        """Point g_config at `cfg`; for the 3-D serial variant ("3s") at a copy
+        in its own layout (friction fields from the config's attributes)."""
+        if self.kind == "3s":
+            cfg = T.serial_config(cfg)
         self._cfg_ref = cfg
         C.c_void_p.in_dll(self.lib, "g_config").value = C.addressof(cfg)
 

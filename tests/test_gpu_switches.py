@@ -197,3 +197,37 @@ def test_surface_tension_stages_bitexact(dim):
             g = s.download()
         assert np.any(ho.view["acc"] != 0.0), stage
         assert np.array_equal(g["acc"], ho.view["acc"]), stage
+
+
+@pytest.mark.parametrize("theta", [90.0, 60.0])
+def test_friction_step_matches_oracle(theta):
+    """The contact-line friction of the 3-D serial variant (mps_fluid3D
+    operators.c:337-492; the oracle's restatement is pinned to that build by
+    tests/test_oracle_pin.py): a full step from the same state and list,
+    lists, densities, flags and types bit for bit, pressure within 1e-8,
+    velocity 1e-10, position 1e-14."""
+    _cuda()
+    from mps_b200.session import Session
+    from oracle.pyoracle import Oracle
+    orc = Oracle(3)
+    wl = W.small_dambreak3d(l0=0.02, seed=23, friction_enabled=1, wetting_angle_SL=theta)
+    orc.set_friction(wl.config())
+    try:
+        cfg, hp, nl, cl = _moved(wl, orc)
+        m = cfg.max_neighbors
+        hg = hp.copy()
+        nb_prev, cnt_prev = nl.neighbors[: hp.n * m].copy(), nl.count[: hp.n].copy()
+        assert orc.step(hp, nl, cl, cfg) == 0
+    finally:
+        orc.set_friction(W.small_dambreak3d(l0=0.02, seed=23).config())
+    with Session(cfg, 3, hg.n) as s:
+        s.upload(hg)
+        s.set_initial_params(hp.ps.n0, hp.ps.lambda_, hp.ps.n0_count)
+        s.step_with_list(nb_prev, cnt_prev, m)
+        g = s.download()
+    o = hp.view
+    for f in ("n", "on_surface", "type"):
+        assert np.array_equal(g[f], o[f]), f
+    assert _rel(g["pressure"], o["pressure"]) < P_TOL, _rel(g["pressure"], o["pressure"])
+    assert _rel(g["vel"], o["vel"]) < V_TOL
+    assert _rel(g["pos"], o["pos"]) < X_TOL

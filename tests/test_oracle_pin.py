@@ -190,3 +190,41 @@ def test_oracle_bitexact_surface_tension(dim, kind, theta, oracle3, oracle2):
             assert np.array_equal(hp_o.view[f], hp_r.view[f]), (s, f)
         assert np.array_equal(nl_o.count, nl_r.count)
     ref.lib.cell_list_free(cl_r)
+
+
+@pytest.mark.parametrize("theta", [90.0, 60.0])
+def test_oracle_bitexact_friction(theta, oracle3):
+    """The hybrid friction of the 3-D serial variant (mps_fluid3D
+    operators.c:337-492, applied between the velocity and position updates,
+    simulation.c:52-53): the oracle with its friction parameters set equals
+    the serial reference build (oracle/_ref/libref3s.so, its own SimConfig
+    layout) field for field over several steps, and friction changes the
+    velocities against a run without it."""
+    ref = reference_lib("3s")
+    sw = dict(friction_enabled=1, wetting_angle_SL=theta, friction_velocity_threshold=0.01)
+    wl = W.small_dambreak3d(l0=0.025, seed=8, **sw)
+    cfg = wl.config()
+    assert cfg.friction_enabled == 1
+    oracle3.set_friction(cfg)
+    try:
+        hp_o, nl_o, cl_o = _setup(oracle3, wl, cfg)
+        hp_r = T.HostParticles(3, wl.pos, wl.vel, wl.types)
+        ref.set_config(cfg)
+        ref.lib.particle_system_calc_initial_params(C.byref(hp_r.ps))
+        re = CF.neighbor_radius(cfg)
+        nl_r = T.HostNeighborList(hp_r.n, cfg.max_neighbors)
+        cl_r = ref.cell_list(hp_r.n, re, cfg)
+        ref.lib.neighbor_search_cell_linked_list(C.byref(nl_r.nl), C.byref(hp_r.ps), cl_r, re)
+        for s in range(1, 4):
+            assert oracle3.step(hp_o, nl_o, cl_o, cfg) == 0
+            ref.step(hp_r, nl_r, cl_r, s)
+            for f in FIELDS:
+                assert np.array_equal(hp_o.view[f], hp_r.view[f]), (s, f)
+        ref.lib.cell_list_free(cl_r)
+        oracle3.set_friction(W.small_dambreak3d(l0=0.025, seed=8).config())
+        hp_n, nl_n, cl_n = _setup(oracle3, wl, cfg)
+        for s in range(1, 4):
+            assert oracle3.step(hp_n, nl_n, cl_n, cfg) == 0
+        assert not np.array_equal(hp_n.view["vel"], hp_o.view["vel"])
+    finally:
+        oracle3.set_friction(W.small_dambreak3d(l0=0.025, seed=8).config())
