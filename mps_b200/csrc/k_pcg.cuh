@@ -455,8 +455,9 @@ __global__ void __launch_bounds__(PCG_THREADS, 2) k_pcg(PcgArgs<TM> a)
     bool pend = false;   // p = z + beta p not yet applied
     int pb = 0;          // p lives in a.p (0) or a.p2 (1)
     for (int it = 0; it < a.batch && !done; it++) {
-        if (sqrt(rr) < tol || iter >= maxit) {
+        if (sqrt(rr) < tol || iter >= maxit || isnan(rr)) {   // NaN: see k_cg_spmv
             done = 1;
+            if (isnan(rr)) brk = 1;
             break;
         }
         double *pold = pb ? a.p2 : a.p, *pnew = pb ? a.p : a.p2;

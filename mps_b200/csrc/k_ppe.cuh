@@ -1198,6 +1198,15 @@ __global__ void __launch_bounds__(CG_BLOCK, 8) k_cg_spmv(int n_eq, const int *__
         if (blockIdx.x == 0 && threadIdx.x == 0) sc->done = 1;
         return;
     }
+    // a NaN residual (a blown-up state) stays NaN: the reference would run on
+    // to cg_max_iter and end with the same NaN solution; stop now instead
+    if (isnan(sc->rr)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            sc->done = 1;
+            sc->breakdown = 1;
+        }
+        return;
+    }
     int lane = threadIdx.x % LPR;
     int rows_per_block = CG_BLOCK / LPR;
     double acc = 0.0;
