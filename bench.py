@@ -96,10 +96,12 @@ def host_cores() -> int:
 # CPU: the reference compiled from source (oracle/_ref), bounded sample
 # ---------------------------------------------------------------------------
 
-def reference_cpu_steps(workload: str, steps: int, warmup: int, l0=None, seed: int = 1000):
+def reference_cpu_steps(workload: str, steps: int, warmup: int, l0=None, seed: int = 1000, restart: bool = True):
     """Times `steps` reference simulation_step calls (after `warmup` untimed
     ones) on the workload (the same seeded initial state as the GPU arm's
-    rank 0); returns (fluid particle-steps/s, seconds/step, meta)."""
+    rank 0); with `restart`, every call starts from the initial particles
+    and list, restored between the timed calls, as the GPU arm's steps do.
+    Returns (fluid particle-steps/s, seconds/step, meta)."""
     os.environ.setdefault("OMP_NUM_THREADS", str(host_cores()))
     from mps_b200 import config as CF
     from mps_b200 import types as T
@@ -119,16 +121,30 @@ def reference_cpu_steps(workload: str, steps: int, warmup: int, l0=None, seed: i
     nl = T.HostNeighborList(hp.n, cfg.max_neighbors)
     cl = ref.cell_list(hp.n, re, cfg)
     ref.lib.neighbor_search_cell_linked_list(C.byref(nl.nl), C.byref(hp.ps), cl, re)
+    if restart:
+        arr0, cnt0, nb0 = hp.arr.copy(), nl.count.copy(), nl.neighbors.copy()
+
+    def restore():
+        if restart:
+            hp.arr[:] = arr0
+            nl.count[:] = cnt0
+            nl.neighbors[:] = nb0
+
     for s in range(warmup):
+        restore()
         ref.step(hp, nl, cl, s + 1)
-    t0 = time.perf_counter()
+    dt = 0.0
     for s in range(steps):
+        restore()
+        t0 = time.perf_counter()
         ref.step(hp, nl, cl, warmup + s + 1)
-    dt = time.perf_counter() - t0
+        dt += time.perf_counter() - t0
     ref.lib.cell_list_free(cl)
     meta = {"kind": kind, "cores": int(os.environ["OMP_NUM_THREADS"]),
-            "sample": f"{wl.name} ({wl.n} particles, {wl.n_fluid} fluid), the first {steps} reference "
-                      f"simulation_step call(s) from the initial state after {warmup} warm-up, "
+            "sample": f"{wl.name} ({wl.n} particles, {wl.n_fluid} fluid), {steps} reference "
+                      f"simulation_step call(s) after {warmup} warm-up, "
+                      + ("each from the initial state (restored between calls, not timed), " if restart else
+                         "consecutive from the initial state, ") +
                       "OpenMP build of mps_fluid3D_parallel compiled from source; n0/lambda from the oracle's "
                       "cell-list form of particle_system_calc_initial_params (bit-identical, not timed)"}
     return wl.n_fluid * steps / dt, dt / max(steps, 1), meta
@@ -479,7 +495,7 @@ def run_b200(args, rank: int, world: int, local_rank: int):
                     "others": roof[1:]})
         cpu = None
         if world == 1 and not args.no_cpu:
-            v, sec, meta = reference_cpu_steps(args.workload, args.cpu_steps, 0, l0=args.l0)
+            v, sec, meta = reference_cpu_steps(args.workload, args.cpu_steps, 0, l0=args.l0, restart=args.restart)
             cpu = {"value": v, "unit": UNIT, "cores": meta["cores"], "kind": meta["kind"], "sample": meta["sample"],
                    "seconds_per_step": sec}
         forms_out = {}
@@ -981,7 +997,7 @@ def main():
         if rank != 0:
             return 0
         nsteps = min(args.steps, REF_WINDOW)
-        v, sec, meta = reference_cpu_steps(args.workload, nsteps, 0, l0=args.l0)
+        v, sec, meta = reference_cpu_steps(args.workload, nsteps, 0, l0=args.l0, restart=args.restart)
         meta["sample"] += (f"; a bounded window of {nsteps} step(s) instead of {args.steps} after {args.warmup} "
                            "warm-up (no warm-up: the reference allocates its PPE buffers in every call)")
         line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
