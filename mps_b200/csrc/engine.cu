@@ -304,6 +304,7 @@ private:
     // CTAs per SM the colour sweep is compiled for (MPS_SWEEP_OCC: 6 or 8;
     // 0 = by storage type)
     int sweep_occ_ = 0;
+    int head_rows_ = 1;            // head rows per lane group of the colour sweep (MPS_SWEEP_HR: 1 or 2)
     // polls of the first wait for a staged block inverse (MPS_TEST_MBAR_POLLS
     // lowers it, down to 0, to exercise the timeout path)
     int first_polls_ = MBAR_POLLS;
@@ -462,6 +463,7 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
     }
     if (const char *e = std::getenv("MPS_SWEEP_HB")) head_batch_ = std::atoi(e) == 8 ? 8 : 4;
     if (const char *e = std::getenv("MPS_SWEEP_OCC")) sweep_occ_ = std::atoi(e) == 8 ? 8 : 6;
+    if (const char *e = std::getenv("MPS_SWEEP_HR")) head_rows_ = std::atoi(e) == 2 ? 2 : 1;
     if (const char *e = std::getenv("MPS_PCG_BATCH")) {
         int v = std::atoi(e);
         if (v >= 1 && v <= 1024) pcg_batch_ = v;
@@ -498,6 +500,10 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
     MPS_CUDA(cudaFuncSetAttribute(k_sweep_colour<true, double, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(sizeof(double) * CELL_STAGE_MAX)));
     MPS_CUDA(cudaFuncSetAttribute(k_sweep_colour<false, double, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(double) * CELL_STAGE_MAX)));
+    MPS_CUDA(cudaFuncSetAttribute(k_sweep_colour<true, double, 4, 6, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(double) * CELL_STAGE_MAX)));
+    MPS_CUDA(cudaFuncSetAttribute(k_sweep_colour<false, double, 4, 6, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(sizeof(double) * CELL_STAGE_MAX)));
     alloc_state();
     build_grid();
@@ -1387,10 +1393,16 @@ void Engine<D>::run_sweep(const PcgBufs<TM> &v, bool fwdir)
             colk = fwdir ? k_sweep_colour<true, TM, 4, 8> : k_sweep_colour<false, TM, 4, 8>;
             if (sizeof(TM) == 8) stage = win_ + 824;
         }
+        // two head rows per lane group: half the cross CTAs, each with two
+        // rows' loads in flight (MPS_SWEEP_HR=2)
+        if (head_rows_ == 2) {
+            if (occ == 8) colk = fwdir ? k_sweep_colour<true, TM, 4, 8, 2> : k_sweep_colour<false, TM, 4, 8, 2>;
+            else colk = fwdir ? k_sweep_colour<true, TM, 4, 6, 2> : k_sweep_colour<false, TM, 4, 6, 2>;
+        }
         for (int i = 0; i < nc; i++) {
             int c = order[i], cn = i + 1 < nc ? order[i + 1] : -1;
             int nrb = cn >= 0 ? row_off_[cn] : 0, nre = cn >= 0 ? row_off_[cn + 1] : 0;
-            int ncb = cn >= 0 ? nblk((long long)(nre - nrb) * 8, CELL_THREADS) : 0;
+            int ncb = cn >= 0 ? nblk((long long)(nre - nrb) * 8, CELL_THREADS * head_rows_) : 0;
             lk(2, colk, nwin_[c] + ncb, CELL_THREADS, sizeof(TM) * stage,
                (const int *)wfirst_.p + win_off_[c], nwin_[c], (const int2 *)adesc_.p, (const int *)inv_off_.p,
                fwdir ? v.inv_cm : v.inv_rm, pko, pkl, pkv, pkk, v.dinv, (const int *)(fwdir ? xp_lo_.p : xp_up_.p),

@@ -748,7 +748,7 @@ __global__ void k_gather_colour_offsets(ColourIdx at, int n, const int *__restri
 // dependent: what it loads before pdl_wait() (row bounds, factor values and
 // columns, block inverses, cell descriptors) is written once per step,
 // before the CG loop; x, part and the CG scalars are read only after it.
-template <bool FWD, class TM, int HB = 4, int MINB = 6>
+template <bool FWD, class TM, int HB = 4, int MINB = 6, int HR = 1>
 __global__ void __launch_bounds__(CELL_THREADS, MINB)
 k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict__ desc,
                const int *__restrict__ inv_off, const TM *__restrict__ inv, const int *__restrict__ pk_off,
@@ -763,35 +763,54 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
     __shared__ __align__(8) unsigned long long bar;
     pdl_trigger();
     if ((int)blockIdx.x >= nwin) {
-        // cross CTA: head sums of the next colour's rows
-        int t = (blockIdx.x - nwin) * blockDim.x + threadIdx.x;
-        int r = nrb + t / LPR;
-        int lane = t % LPR;
-        int a = 0, b = 0;
-        if (r < nre) {
-            a = FWD ? __ldg(&xp[r]) : __ldg(&xs[r]);
-            b = FWD ? __ldg(&xs[r]) : __ldg(&xp[r + 1]);
+        // cross CTA: head sums of the next colour's rows, HR rows per group
+        // of LPR lanes (the CTA's groups take GPB consecutive rows per h),
+        // all their first entries loaded before the wait
+        constexpr int GPB = CELL_THREADS / LPR;
+        int blk = blockIdx.x - nwin;
+        int lane = threadIdx.x % LPR;
+        int r[HR], a[HR], b[HR];
+#pragma unroll
+        for (int h = 0; h < HR; h++) {
+            r[h] = nrb + (blk * HR + h) * GPB + threadIdx.x / LPR;
+            a[h] = 0;
+            b[h] = 0;
+            if (r[h] < nre) {
+                a[h] = FWD ? __ldg(&xp[r[h]]) : __ldg(&xs[r[h]]);
+                b[h] = FWD ? __ldg(&xs[r[h]]) : __ldg(&xp[r[h] + 1]);
+            }
         }
         // the first HB entries of each lane in one batch, before the wait
-        TM f[HB];
-        int cc[HB];
+        TM f[HR][HB];
+        int cc[HR][HB];
 #pragma unroll
-        for (int u = 0; u < HB; u++) {
-            int q = a + lane + u * LPR;
-            bool ok = q < b;
-            f[u] = ok ? __ldg(&xf[q]) : TM(0);
-            cc[u] = ok ? __ldg(&xc[q]) : -1;
-        }
+        for (int h = 0; h < HR; h++)
+#pragma unroll
+            for (int u = 0; u < HB; u++) {
+                int q = a[h] + lane + u * LPR;
+                bool ok = q < b[h];
+                f[h][u] = ok ? __ldg(&xf[q]) : TM(0);
+                cc[h][u] = ok ? __ldg(&xc[q]) : -1;
+            }
         pdl_wait();
         if (sc->done) return;
-        T s = T(0);
+        T s[HR];
 #pragma unroll
-        for (int u = 0; u < HB; u++)
-            if (cc[u] >= 0) s += T(f[u]) * x[cc[u]];
-        for (int q = a + lane + HB * LPR; q < b; q += LPR) s += T(__ldg(&xf[q])) * x[__ldg(&xc[q])];
+        for (int h = 0; h < HR; h++) {
+            s[h] = T(0);
 #pragma unroll
-        for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LPR);
-        if (lane == 0 && r < nre) part[r] = rhs[r] - s;
+            for (int u = 0; u < HB; u++)
+                if (cc[h][u] >= 0) s[h] += T(f[h][u]) * x[cc[h][u]];
+        }
+#pragma unroll
+        for (int h = 0; h < HR; h++)
+            for (int q = a[h] + lane + HB * LPR; q < b[h]; q += LPR) s[h] += T(__ldg(&xf[q])) * x[__ldg(&xc[q])];
+#pragma unroll
+        for (int h = 0; h < HR; h++) {
+#pragma unroll
+            for (int o = LPR / 2; o > 0; o >>= 1) s[h] += __shfl_down_sync(0xffffffffu, s[h], o, LPR);
+            if (lane == 0 && r[h] < nre) part[r[h]] = rhs[r[h]] - s[h];
+        }
         return;
     }
     // window CTA
