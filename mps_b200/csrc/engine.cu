@@ -323,6 +323,11 @@ private:
     DevArray<double> A_, F_, b_, x_, r_, z_, p_, Ap_, y_, part_, partials_, p2_;
     DevArray<float> A32_, xf32_lo_, xf32_up_, pkv32_lo_, pkv32_up_, inv32_cm_, inv32_rm_, dinv32_;
     DevArray<double> zprev_, dsum_;
+    DevArray<uint2> ac32_, xfc32_lo_, xfc32_up_;   // packed FP32 matrix and cross runs (mixed form)
+    // mixed form: the FP32 matrix and cross runs as packed 8-byte words (1,
+    // default) or as separate value and column arrays (0; MPS_PACK)
+    int pack_ = 1;
+    bool packed_ = false;   // the last mixed solve used the packed words
     DevArray<CGScalars> sc_;
     DevArray<unsigned> ticket_, err_;
     int n_eq_ = 0;
@@ -406,6 +411,9 @@ private:
         const double *b;
         const double *A64 = nullptr;   // if set, the SpMV reads this FP64 matrix instead of A
         const double *dsum = nullptr;  // if set, the SpMV is in difference form with these row sums
+        // FP32 only: packed (value bits, column) words of the matrix and of
+        // the cross runs; if set, the SpMV and the colour sweeps read these
+        const uint2 *ac = nullptr, *xfc_lo = nullptr, *xfc_up = nullptr;
     };
     template <class TM>
     void pcg_solve(const PcgBufs<TM> &v, double tol, int maxit, bool icc, int n_eq, long long nnz,
@@ -460,6 +468,7 @@ Engine<D>::Engine(const mps_params_t &p, int capacity)
         if (v > 0.0 && v < 1.0) rel_delta_ = v;
     }
     if (const char *e = std::getenv("MPS_MIXED_SPMV")) mixed_spmv_ = std::atoi(e);
+    if (const char *e = std::getenv("MPS_PACK")) pack_ = std::atoi(e) ? 1 : 0;
     if (const char *e = std::getenv("MPS_SWEEP")) {
         int v = std::atoi(e);
         sweep_mode_ = (v == 0 || v == 1) ? v : 2;
@@ -1402,6 +1411,19 @@ void Engine<D>::run_sweep(const PcgBufs<TM> &v, bool fwdir)
             if (occ == 8) colk = fwdir ? k_sweep_colour<true, TM, 4, 8, 2> : k_sweep_colour<false, TM, 4, 8, 2>;
             else colk = fwdir ? k_sweep_colour<true, TM, 4, 6, 2> : k_sweep_colour<false, TM, 4, 6, 2>;
         }
+        // the FP32 cross runs as packed words
+        if constexpr (sizeof(TM) == 4) {
+            if (v.xfc_lo) {
+                if (occ == 8 && head_rows_ == 2)
+                    colk = fwdir ? k_sweep_colour<true, TM, 4, 8, 2, true> : k_sweep_colour<false, TM, 4, 8, 2, true>;
+                else if (occ == 8)
+                    colk = fwdir ? k_sweep_colour<true, TM, 4, 8, 1, true> : k_sweep_colour<false, TM, 4, 8, 1, true>;
+                else if (head_rows_ == 2)
+                    colk = fwdir ? k_sweep_colour<true, TM, 4, 6, 2, true> : k_sweep_colour<false, TM, 4, 6, 2, true>;
+                else
+                    colk = fwdir ? k_sweep_colour<true, TM, 4, 6, 1, true> : k_sweep_colour<false, TM, 4, 6, 1, true>;
+            }
+        }
         for (int i = 0; i < nc; i++) {
             int c = order[i], cn = i + 1 < nc ? order[i + 1] : -1;
             int nrb = cn >= 0 ? row_off_[cn] : 0, nre = cn >= 0 ? row_off_[cn + 1] : 0;
@@ -1411,7 +1433,7 @@ void Engine<D>::run_sweep(const PcgBufs<TM> &v, bool fwdir)
                fwdir ? v.inv_cm : v.inv_rm, pko, pkl, pkv, pkk, v.dinv, (const int *)(fwdir ? xp_lo_.p : xp_up_.p),
                (const int *)(fwdir ? xs_lo_.p : xs_up_.p), (const int *)(fwdir ? xc_lo_.p : xc_up_.p),
                fwdir ? v.xf_lo : v.xf_up, (int)(i == 0), nrb, nre, rhs, v.part, out, (const CGScalars *)sc_.p,
-               stage, first_polls_, err_.p);
+               stage, first_polls_, err_.p, fwdir ? v.xfc_lo : v.xfc_up);
         }
     }
 }
@@ -1453,22 +1475,32 @@ void Engine<D>::pcg_solve(const PcgBufs<TM> &v, double tol, int maxit, bool icc,
         const int *rp = row_ptr_.p, *ci = col_.p;
         if (v.A64)
             lk(4, k_cg_spmv<8, double>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A64, (const T *)v.p, v.Ap, partials_.p,
-               ticket_.p, sc_.p, (const double *)nullptr);
+               ticket_.p, sc_.p, (const double *)nullptr, (const uint2 *)nullptr);
+        else if (v.dsum && v.ac) {
+            if constexpr (sizeof(TM) == 4) {
+                if (lpr == 16)
+                    lk(4, k_cg_spmv<16, TM, true, true>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap,
+                       partials_.p, ticket_.p, sc_.p, v.dsum, v.ac);
+                else
+                    lk(4, k_cg_spmv<8, TM, true, true>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap,
+                       partials_.p, ticket_.p, sc_.p, v.dsum, v.ac);
+            }
+        }
         else if (v.dsum && lpr == 16)
             lk(4, k_cg_spmv<16, TM, true>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
-               ticket_.p, sc_.p, v.dsum);
+               ticket_.p, sc_.p, v.dsum, (const uint2 *)nullptr);
         else if (v.dsum)
             lk(4, k_cg_spmv<8, TM, true>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
-               ticket_.p, sc_.p, v.dsum);
+               ticket_.p, sc_.p, v.dsum, (const uint2 *)nullptr);
         else if (lpr == 16)
             lk(4, k_cg_spmv<16, TM>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
-               ticket_.p, sc_.p, (const double *)nullptr);
+               ticket_.p, sc_.p, (const double *)nullptr, (const uint2 *)nullptr);
         else if (lpr == 32)
             lk(4, k_cg_spmv<32, TM>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
-               ticket_.p, sc_.p, (const double *)nullptr);
+               ticket_.p, sc_.p, (const double *)nullptr, (const uint2 *)nullptr);
         else
             lk(4, k_cg_spmv<8, TM>, RB, CG_BLOCK, 0, n_eq, rp, ci, v.A, (const T *)v.p, v.Ap, partials_.p,
-               ticket_.p, sc_.p, (const double *)nullptr);
+               ticket_.p, sc_.p, (const double *)nullptr, (const uint2 *)nullptr);
     };
     const bool persist = icc && sweep_mode_ == 2;
     if (icc) {
@@ -1727,18 +1759,37 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
 {
     const int RB = RED_BLOCKS;
     size_t nz = (size_t)nnz;
+    // packed words for the launch-per-colour loop; the persistent and the
+    // CTA-per-cell loops read the separate arrays
+    const bool pk = pack_ && sweep_mode_ == 0 && head_batch_ == 4;
+    const bool pk_spmv = pk && mixed_spmv_ == 2;
     for (auto *v : {&A32_, &pkv32_lo_, &pkv32_up_}) v->reserve(nz);
     xf32_lo_.reserve((size_t)nx_lo_ + 1);
     xf32_up_.reserve((size_t)nx_up_ + 1);
     for (auto *v : {&inv32_cm_, &inv32_rm_}) v->reserve((size_t)ninv_ + 1);
     dinv32_.reserve((size_t)cap_);
     zprev_.reserve((size_t)cap_);
-    launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)A_.p, A32_.p);
+    if (pk_spmv) {
+        ac32_.reserve(nz);
+        launch(k_pack_fc, RB, CG_BLOCK, 0, st_, nz, (const double *)A_.p, (const int *)col_.p, ac32_.p);
+    } else
+        launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)A_.p, A32_.p);
+    if (icc && pk) {
+        xfc32_lo_.reserve((size_t)nx_lo_ + 1);
+        xfc32_up_.reserve((size_t)nx_up_ + 1);
+        launch(k_pack_fc, RB, CG_BLOCK, 0, st_, (size_t)nx_lo_, (const double *)xf_lo_.p, (const int *)xc_lo_.p,
+               xfc32_lo_.p);
+        launch(k_pack_fc, RB, CG_BLOCK, 0, st_, (size_t)nx_up_, (const double *)xf_up_.p, (const int *)xc_up_.p,
+               xfc32_up_.p);
+    }
+    packed_ = icc && pk;
     if (icc) {
-        launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, (size_t)nx_lo_, (const double *)xf_lo_.p,
-               xf32_lo_.p);
-        launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, (size_t)nx_up_, (const double *)xf_up_.p,
-               xf32_up_.p);
+        if (!pk) {
+            launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, (size_t)nx_lo_, (const double *)xf_lo_.p,
+                   xf32_lo_.p);
+            launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, (size_t)nx_up_, (const double *)xf_up_.p,
+                   xf32_up_.p);
+        }
         launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)pk_val_lo_.p, pkv32_lo_.p);
         launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, nz, (const double *)pk_val_up_.p, pkv32_up_.p);
         launch(k_convert<double, float>, RB, CG_BLOCK, 0, st_, (size_t)n_eq, (const double *)dinv_.p, dinv32_.p);
@@ -1761,6 +1812,11 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
                      inv32_rm_.p, x_.p,       r_.p,       z_.p,        p_.p,        Ap_.p,     y_.p,
                      part_.p,     b_.p};
     if (mixed_spmv_ == 1 && sweep_mode_ != 2) v.A64 = A_.p;   // tuning alternatives of the inner SpMV
+    if (pk_spmv) v.ac = ac32_.p;
+    if (packed_) {
+        v.xfc_lo = xfc32_lo_.p;
+        v.xfc_up = xfc32_up_.p;
+    }
     if (mixed_spmv_ == 2) {
         dsum_.reserve((size_t)cap_);
         launch(k_row_sum, nblk(n_eq, TPB), TPB, 0, st_, n_eq, (const int *)row_ptr_.p, (const double *)A_.p,
@@ -2262,6 +2318,10 @@ void Engine<D>::apply_preconditioner(const double *r, double *z)
         PcgBufs<float> v{A32_.p,      xf32_lo_.p, xf32_up_.p, pkv32_lo_.p, pkv32_up_.p, dinv32_.p, inv32_cm_.p,
                          inv32_rm_.p, x_.p,       r_.p,       z_.p,        p_.p,        Ap_.p,     y_.p,
                          part_.p,     b_.p};
+        if (packed_) {
+            v.xfc_lo = xfc32_lo_.p;
+            v.xfc_up = xfc32_up_.p;
+        }
         if (sweep_mode_ == 2) launch_pcg<float>(v, true, 0);
         else {
             run_sweep<float>(v, true);

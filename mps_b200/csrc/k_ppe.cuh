@@ -730,6 +730,38 @@ __global__ void k_gather_colour_offsets(ColourIdx at, int n, const int *__restri
     if (t < n) out[t] = inv_off[at.k[t]];
 }
 
+// ---- packed FP32 entries -------------------------------------------------------
+//
+// The mixed form's FP32 matrix and cross runs can be stored as one 8-byte
+// word per entry (the value's bits, the column): one load per entry instead
+// of a 4-byte value load and a 4-byte column load, so a warp's load request
+// moves as many bytes as an FP64 value load does.
+
+// out[i] = (bits of (float)val[i], col[i]): the FP32 value rounds to
+// nearest, as k_convert<double, float> does.
+__global__ void k_pack_fc(size_t n, const double *__restrict__ val, const int *__restrict__ col,
+                          uint2 *__restrict__ out)
+{
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = make_uint2(__float_as_uint((float)val[i]), (unsigned)col[i]);
+}
+
+// Entry q of a run (value v, column k): from the packed words when PK, else
+// from the value and column arrays; (0, -1) when !ok.
+template <class TM, bool PK>
+__device__ __forceinline__ void load_entry(const TM *__restrict__ f, const int *__restrict__ c,
+                                           const uint2 *__restrict__ fc, int q, bool ok, TM &v, int &k)
+{
+    if (PK) {
+        uint2 e = ok ? __ldg(&fc[q]) : make_uint2(0u, 0xffffffffu);
+        v = TM(__uint_as_float(e.x));
+        k = (int)e.y;
+    } else {
+        v = ok ? __ldg(&f[q]) : TM(0);
+        k = ok ? __ldg(&c[q]) : -1;
+    }
+}
+
 // ---- one launch per colour ---------------------------------------------------
 //
 // k_sweep_colour finishes colour c and starts the next colour of the sweep
@@ -748,14 +780,17 @@ __global__ void k_gather_colour_offsets(ColourIdx at, int n, const int *__restri
 // dependent: what it loads before pdl_wait() (row bounds, factor values and
 // columns, block inverses, cell descriptors) is written once per step,
 // before the CG loop; x, part and the CG scalars are read only after it.
-template <bool FWD, class TM, int HB = 4, int MINB = 6, int HR = 1>
+// PK (FP32 only): the cross entries come from the packed words xfc instead of
+// xf and xc, with the same sums in the same order.
+template <bool FWD, class TM, int HB = 4, int MINB = 6, int HR = 1, bool PK = false>
 __global__ void __launch_bounds__(CELL_THREADS, MINB)
 k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict__ desc,
                const int *__restrict__ inv_off, const TM *__restrict__ inv, const int *__restrict__ pk_off,
                const int *__restrict__ pk_len, const TM *__restrict__ pk_val, const unsigned char *__restrict__ pk_k,
                const TM *__restrict__ dinv, const int *__restrict__ xp, const int *__restrict__ xs,
                const int *__restrict__ xc, const TM *__restrict__ xf, int first, int nrb, int nre, const double *rhs,
-               double *part, double *x, const CGScalars *sc, int stage_elems, int first_polls, unsigned *err)
+               double *part, double *x, const CGScalars *sc, int stage_elems, int first_polls, unsigned *err,
+               const uint2 *__restrict__ xfc = nullptr)
 {
     using T = double;   // vectors and sums; TM is the storage type of the factor
     constexpr int LPR = 8;
@@ -788,9 +823,7 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
 #pragma unroll
             for (int u = 0; u < HB; u++) {
                 int q = a[h] + lane + u * LPR;
-                bool ok = q < b[h];
-                f[h][u] = ok ? __ldg(&xf[q]) : TM(0);
-                cc[h][u] = ok ? __ldg(&xc[q]) : -1;
+                load_entry<TM, PK>(xf, xc, xfc, q, q < b[h], f[h][u], cc[h][u]);
             }
         pdl_wait();
         if (sc->done) return;
@@ -804,7 +837,12 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
         }
 #pragma unroll
         for (int h = 0; h < HR; h++)
-            for (int q = a[h] + lane + HB * LPR; q < b[h]; q += LPR) s[h] += T(__ldg(&xf[q])) * x[__ldg(&xc[q])];
+            for (int q = a[h] + lane + HB * LPR; q < b[h]; q += LPR) {
+                TM fv;
+                int k;
+                load_entry<TM, PK>(xf, xc, xfc, q, true, fv, k);
+                s[h] += T(fv) * x[k];
+            }
 #pragma unroll
         for (int h = 0; h < HR; h++) {
 #pragma unroll
@@ -853,14 +891,17 @@ k_sweep_colour(const int *__restrict__ wfirst, int nwin, const int2 *__restrict_
 #pragma unroll
                 for (int u = 0; u < TB; u++) {
                     int q = a + lane + u * TL;
-                    bool ok = q < e;
-                    tf[u] = ok ? __ldg(&xf[q]) : TM(0);
-                    tc[u] = ok ? __ldg(&xc[q]) : -1;
+                    load_entry<TM, PK>(xf, xc, xfc, q, q < e, tf[u], tc[u]);
                 }
 #pragma unroll
                 for (int u = 0; u < TB; u++)
                     if (tc[u] >= 0) s += T(tf[u]) * x[tc[u]];
-                for (int q = a + lane + TB * TL; q < e; q += TL) s += T(__ldg(&xf[q])) * x[__ldg(&xc[q])];
+                for (int q = a + lane + TB * TL; q < e; q += TL) {
+                    TM fv;
+                    int k;
+                    load_entry<TM, PK>(xf, xc, xfc, q, true, fv, k);
+                    s += T(fv) * x[k];
+                }
             }
             s += __shfl_down_sync(0xffffffffu, s, 1, TL);
             if (lane == 0 && r < R1) part[r] = (first ? rhs[r] : part[r]) - s;
@@ -1202,11 +1243,13 @@ constexpr int SPMV_U = 8;   // entries per lane loaded in one batch by the FP32 
 // to FP32 then perturbs the product in proportion to the differences of p
 // across a pair, not to |A_ij| |p_j|, whose cancellation in a Laplacian row
 // would amplify the rounding by orders of magnitude.
-template <int LPR, class TM, bool DIFF = false>
+// PK (FP32 only): the entries come from the packed words ac instead of A and
+// col, with the same sums in the same order.
+template <int LPR, class TM, bool DIFF = false, bool PK = false>
 __global__ void __launch_bounds__(CG_BLOCK, 8) k_cg_spmv(int n_eq, const int *__restrict__ row_ptr, const int *__restrict__ col,
                           const TM *__restrict__ A, const double *p, double *Ap,
                           double *partials, unsigned *ticket, CGScalars *sc,
-                          const double *__restrict__ dsum = nullptr)
+                          const double *__restrict__ dsum = nullptr, const uint2 *__restrict__ ac = nullptr)
 {
     using T = double;   // vectors and sums; TM is the storage type of the matrix
     __shared__ double sh[CG_BLOCK / 32];
@@ -1248,16 +1291,20 @@ __global__ void __launch_bounds__(CG_BLOCK, 8) k_cg_spmv(int n_eq, const int *__
 #pragma unroll
             for (int u = 0; u < SPMV_U; u++) {
                 int q = q0 + u * LPR;
-                bool ok = q < q1;
-                a[u] = ok ? __ldg(&A[q]) : TM(0);
-                c[u] = ok ? __ldg(&col[q]) : -1;
+                a[u] = TM(0);
+                c[u] = -1;
+                if (q < q1) load_entry<TM, PK>(A, col, ac, q, true, a[u], c[u]);
             }
             T pi = DIFF ? p[r] : T(0);
 #pragma unroll
             for (int u = 0; u < SPMV_U; u++)
                 if (c[u] >= 0) s += T(a[u]) * (DIFF ? p[c[u]] - pi : p[c[u]]);
-            for (int q = q0 + SPMV_U * LPR; q < q1; q += LPR)
-                s += T(__ldg(&A[q])) * (DIFF ? p[__ldg(&col[q])] - pi : p[__ldg(&col[q])]);
+            for (int q = q0 + SPMV_U * LPR; q < q1; q += LPR) {
+                TM av;
+                int k;
+                load_entry<TM, PK>(A, col, ac, q, true, av, k);
+                s += T(av) * (DIFF ? p[k] - pi : p[k]);
+            }
         }
 #pragma unroll
         for (int o = LPR / 2; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o, LPR);

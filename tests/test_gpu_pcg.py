@@ -14,6 +14,12 @@ Checked through the C ABI:
     recursive residual creeps along the tolerance, so there 10 %);
   * two runs of the persistent kernel are bit-identical (fixed-order grid
     sums, same grid);
+  * the mixed form's FP32 matrix and cross runs read as packed (value,
+    column) words (MPS_PACK=1, the default) or as separate arrays
+    (MPS_PACK=0): the same sums in the same order, so bit-identical
+    pressures, positions and iteration counts over three steps, on the
+    dam break and on a densely packed column (unstaged and substituted
+    cells);
   * the grid barrier's bounded wait: with the poll limit lowered to zero
     (MPS_TEST_BAR_POLLS=0) the barrier gives up at once, the kernel returns
     and the step fails with MPS_ERR_CUDA; the device stays usable and a
@@ -39,9 +45,10 @@ def _rel(a, b):
     return np.linalg.norm(a - b) / (nb if nb > 0 else 1.0)
 
 
-def _run(monkeypatch, sweep, wl, steps, precision=0):
+def _run(monkeypatch, sweep, wl, steps, precision=0, pack="1"):
     from mps_b200.session import start
     monkeypatch.setenv("MPS_SWEEP", sweep)
+    monkeypatch.setenv("MPS_PACK", pack)
     hp = T.HostParticles(wl.dim, wl.pos, wl.vel, wl.types)
     s = start(wl.config(), wl.dim, hp, precision=precision)
     its = []
@@ -82,6 +89,21 @@ def test_persistent_pcg_is_deterministic(monkeypatch):
     assert np.array_equal(ia, ib)
     assert np.array_equal(ga["pressure"], gb["pressure"])
     assert np.array_equal(ga["pos"], gb["pos"])
+
+
+@pytest.mark.parametrize("case", ["dambreak3d", "dense3d"])
+def test_packed_fp32_entries_are_bit_identical(case, monkeypatch):
+    _cuda()
+    if case == "dense3d":
+        wl = W.small_dambreak3d(l0=0.014, seed=5, influence_ratio_lap="4.43")
+    else:
+        wl = W.dambreak("c1", l0=0.02, seed=3)
+    ga, ia = _run(monkeypatch, "0", wl, 3, precision=1, pack="1")
+    gb, ib = _run(monkeypatch, "0", wl, 3, precision=1, pack="0")
+    assert np.array_equal(ia, ib), (ia, ib)
+    assert np.array_equal(ga["pressure"], gb["pressure"])
+    assert np.array_equal(ga["pos"], gb["pos"])
+    assert np.array_equal(ga["vel"], gb["vel"])
 
 
 def test_grid_barrier_timeout_is_reported(monkeypatch):
