@@ -38,7 +38,7 @@ extern "C" {
 #define MPS_PREC_FP64  0   /* the reference's arithmetic, FP64 everywhere */
 #define MPS_PREC_MIXED 1   /* PPE matrix and IC(0) factor stored in FP32 (SpMV in difference
                               form), FP64 vectors, dot products, refinement residuals and
-                              everything outside the PPE solve */
+                              everything outside the PPE solve; the adjoint PPE solve too */
 
 /* PPE unknown orderings for the IC(0) preconditioner. */
 #define MPS_ORDER_BLOCK_COLOR 0  /* cells as blocks, 2^dim colours (default) */
@@ -315,7 +315,9 @@ int  mps_run_stage(mps_session *s, int stage, const int *neighbors, const int *c
  * collision partners, order and branches, free-surface flags, the PPE
  * unknown set, the P_min argument, ghosting); the PPE adjoint is a second
  * ICCG solve with the step's matrix and IC(0) factor to relative residual
- * 1e-12.  Walls, dummies and ghosts get zero adjoints.  Supported: hs_mode
+ * 1e-12 (in the session's precision form: with MPS_PREC_MIXED, the mixed
+ * solve with reliable updates, to 1e-12 or the FP64 rounding floor if
+ * that is higher).  Walls, dummies and ghosts get zero adjoints.  Supported: hs_mode
  * 0, ppe_type 0, cmps_gradient 0, no pressure clamp; other switches return
  * MPS_ERR_UNSUPPORTED, as do more than 8 collision impulses on one
  * particle in one step.  mps_adjoint_get reads the current seeds (NULL

@@ -426,7 +426,9 @@ private:
     void launch_pcg(const PcgBufs<TM> &v, bool apply, int batch);
     int pcg_grid(const void *kernel);
     void trace_phases(int iterations);
-    void mixed_solve(int n_eq, long long nnz, bool icc);
+    // adjoint: stop at kAdjRtol ||b|| (or the rounding floor) and leave the
+    // step's metrics as they are
+    void mixed_solve(int n_eq, long long nnz, bool icc, bool adjoint = false);
     void build_windows(bool fp32);
     static constexpr int kMaxUpdates = 200;      // reliable updates of the mixed form, at most
     static constexpr double kDelta = 0.01;       // residual reduction between reliable updates (mixed form)
@@ -1755,7 +1757,7 @@ void Engine<D>::build_windows(bool fp32)
 // roundoff: kFloor times the rounding floor of an FP64 residual, where the
 // FP64 form's own solve ends; or when the true residual stalls.
 template <int D>
-void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
+void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc, bool adjoint)
 {
     const int RB = RED_BLOCKS;
     size_t nz = (size_t)nnz;
@@ -1805,7 +1807,8 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
     MPS_CUDA(cudaMemcpyAsync(sc_host_, sc_.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, st_));
     MPS_CUDA(cudaStreamSynchronize(st_));
     double bnorm = std::sqrt(sc_host_->rr_outer);
-    double target = std::max(prm_.cg_tolerance, std::max(prm_.refine_tolerance, 0.0) * bnorm);
+    double target = adjoint ? kAdjRtol * bnorm
+                            : std::max(prm_.cg_tolerance, std::max(prm_.refine_tolerance, 0.0) * bnorm);
     double rnorm = bnorm, rbest = bnorm, floor_norm = 0.0;
     int updates = 0, stalls = 0;
     PcgBufs<float> v{A32_.p,      xf32_lo_.p, xf32_up_.p, pkv32_lo_.p, pkv32_up_.p, dinv32_.p, inv32_cm_.p,
@@ -1851,6 +1854,7 @@ void Engine<D>::mixed_solve(int n_eq, long long nnz, bool icc)
         }
     }
     int inner = sc_host_->iter;
+    if (adjoint) return;
     met.ppe_iterations = inner;
     met.ppe_outer = updates;
     met.ppe_residual = rnorm;
@@ -2094,11 +2098,19 @@ void Engine<D>::step_adjoint()
         if (bnorm > 0.0) {
             launch(k_adj_scale, RB, CG_BLOCK, 0, st_, n_eq, b_.p, 1.0 / bnorm);
             bool icc = prm_.solver_type == 1;
-            PcgBufs<double> v{A_.p,      xf_lo_.p, xf_up_.p, pk_val_lo_.p, pk_val_up_.p, dinv_.p, inv_cm_.p,
-                              inv_rm_.p, x_.p,     r_.p,     z_.p,         p_.p,         Ap_.p,   y_.p,
-                              part_.p,   b_.p};
-            if (icc && sweep_mode_ == 0) build_windows(false);   // FP64 sweeps: FP64 windows
-            pcg_solve<double>(v, kAdjRtol, prm_.cg_max_iter, icc, n_eq, nnz_);
+            if (prm_.precision == MPS_PREC_MIXED) {
+                // the mixed form's solve (FP32 matrix and factor, FP64
+                // vectors, reliable updates) down to the same relative
+                // residual, or to the FP64 rounding floor if that is higher
+                if (icc && sweep_mode_ == 0) build_windows(true);
+                mixed_solve(n_eq, nnz_, icc, true);
+            } else {
+                PcgBufs<double> v{A_.p,      xf_lo_.p, xf_up_.p, pk_val_lo_.p, pk_val_up_.p, dinv_.p, inv_cm_.p,
+                                  inv_rm_.p, x_.p,     r_.p,     z_.p,         p_.p,         Ap_.p,   y_.p,
+                                  part_.p,   b_.p};
+                if (icc && sweep_mode_ == 0) build_windows(false);   // FP64 sweeps: FP64 windows
+                pcg_solve<double>(v, kAdjRtol, prm_.cg_max_iter, icc, n_eq, nnz_);
+            }
             launch(k_adj_mu, RB, CG_BLOCK, 0, st_, n_eq, (const int *)part_of_row_.p, (const int *)S().id,
                    (const double *)x_.p, bnorm, adj_.mu);
         }
