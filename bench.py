@@ -465,8 +465,9 @@ def run_b200(args, rank: int, world: int, local_rank: int):
             fwd_ms = pm["prof_fwd_ms"] / max(pm["prof_fwd_sweeps"], 1)
             bwd_ms = pm["prof_bwd_ms"] / max(pm["prof_bwd_sweeps"], 1)
             vec_ms = pm["prof_vec_ms"] / max(pm["prof_iterations"], 1)
-            # SpMV: matrix value + column per nonzero, row pointer, p and Ap per row (FP64)
-            spmv_b = ((4.0 if fp32 else 8.0) + 4.0) * nnz_mean + 20.0 * rows_mean
+            # SpMV: matrix value + column per nonzero, row pointer, p and Ap per row (FP64),
+            # and in the mixed form's difference form the FP64 row sum
+            spmv_b = ((4.0 if fp32 else 8.0) + 4.0) * nnz_mean + (28.0 if fp32 else 20.0) * rows_mean
             sb = sweep_bytes(pm, fp32)
             sw_b = 0.5 * (sb["forward"] + sb["backward"])
             sw_ms = 0.5 * (fwd_ms + bwd_ms)
